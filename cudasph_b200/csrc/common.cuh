@@ -1,0 +1,92 @@
+// common.cuh -- shared device types and helpers of the sm_100a SPH step.
+//
+// Data layout in HBM (all arrays in tree order = Morton order after sorting):
+//   pos   double4 {x, y, z, range}     range = 2h (the reference's bodies_pos)
+//   vel   double4 {vx, vy, vz, m}      (bodies_vel)
+//   hyd   double4 {rho, P, u, mu}      (hydro_data)
+//   dd    double4 {divv, curlv, omega, psi}  (dots_data)
+//   dots  double4 {ax, ay, az, du}     (bodies_dots, total after gravity)
+//   grav  double4 {gx, gy, gz, phi}    (grav_data)
+//   vsig  double                       (hydro_data2.x)
+//   id    int     original particle index of each slot
+// A gather of one neighbour reads whole 32-byte records (two 16-byte loads).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/cudasph_b200.h"
+
+namespace sph {
+
+constexpr int kLeaf = 32;        // particles per tree leaf = one warp
+constexpr int kFan = 32;         // children per internal node = one warp
+constexpr int kMaxLevels = 8;    // supports up to 32^8 leaves
+constexpr int kStack = 256;      // per-warp traversal stack (entries)
+
+// Device-side view of the tree over Morton-ordered leaves.  Level 0 holds
+// the leaves, level top the single root.  Each box is stored as two float4
+// (lo.xyz, hi.xyz) rounded outward from the FP64 extrema, so that box tests
+// are conservative and the exact FP64 predicate decides membership.
+struct TreeView {
+  int n;                       // particles
+  int levels;                  // number of levels (top = levels - 1)
+  int count[kMaxLevels];       // nodes per level
+  long long base[kMaxLevels];  // offset of each level in lo/hi
+  const float4 *lo;
+  const float4 *hi;
+};
+
+// All per-particle state arrays (one buffer set).
+struct Fields {
+  double4 *pos, *vel, *hyd, *dd, *dots, *grav;
+  double *vsig;
+  int *id;
+};
+
+// arguments of the density / hydro kernels (both precision forms)
+struct HydroArgs {
+  int n, nleaf, cap;
+  const double4 *pos, *vel;
+  double4 *hyd, *dd, *dots;
+  double *vsig;
+  const int *n_ngb, *list;
+  double *ngb_acc;  // optional, list layout: m_i * acc per pair
+  double alpha, beta, gamma;
+  int use_psi;
+  int jside;  // 1: add the j-side pair force with atomics; 0: leave it to the caller
+};
+
+struct StepScalars {
+  // [0] dt_old  [1] dt_new  [2] time  [3..] statistics (SPH_NSTATS)
+  double v[4 + SPH_NSTATS];
+};
+
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+
+__device__ __forceinline__ double4 ld4(const double4 *p) {
+  // two 16-byte read-only loads of one 32-byte record
+  const double2 *q = reinterpret_cast<const double2 *>(p);
+  double2 a = __ldg(q), b = __ldg(q + 1);
+  return make_double4(a.x, a.y, b.x, b.y);
+}
+
+// Exact neighbour predicate, evaluated without contraction so the tree walk
+// reproduces (dx*dx + dy*dy) + dz*dz < range*range bit for bit
+// (dev_find_ngb.cu:66-67 in FP64).
+__device__ __forceinline__ double ds2_exact(double dx, double dy, double dz) {
+  return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+}
+
+__device__ __forceinline__ void raise_flag(unsigned *flags, unsigned f) { atomicOr(flags, f); }
+
+}  // namespace sph
+
+#define SPH_CUDA_TRY(expr)                                       \
+  do {                                                           \
+    cudaError_t err__ = (expr);                                  \
+    if (err__ != cudaSuccess) return sph_internal_cuda_fail(err__, #expr, __FILE__, __LINE__); \
+  } while (0)
+
+int sph_internal_cuda_fail(cudaError_t err, const char *what, const char *file, int line);
+void sph_internal_set_error(const char *msg);

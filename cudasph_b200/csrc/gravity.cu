@@ -1,0 +1,356 @@
+// gravity.cu -- softened direct-N self-gravity (sph_grav_kernel.cu:14-195).
+//
+// Each block owns an i-tile of kThreads * R consecutive (Morton-ordered)
+// particles, R per thread held in registers; the sources stream through
+// shared memory in j-tiles of kThreads records, each record read once per
+// block and broadcast to the R i-particles of every thread.  The inner loop
+// runs on the FP64 pipe (plain form) or on the FP32 FMA pipe (mixed form).
+//
+// Mixed form: all positions of a block are taken relative to an FP64 anchor
+// (the first particle of the i-tile) and rounded to FP32 once per j per
+// block, so a close pair keeps the relative accuracy of FP32 on its small
+// separation.  Each thread sums a j-tile's contributions in FP32 and folds
+// the tile partial into a compensated (Kahan-Babuska) float-float
+// accumulator, the counterpart of the reference's float-float `dreal`
+// accumulation (dreal.h:4-127).
+//
+// Softening: Plummer (r^2 + eps^2) or the reference's M4-spline softening at
+// the smoothing ranges of i and j with half contributions
+// (sph_grav_kernel.cu:32-105); the spline branch is taken only by pairs
+// closer than max(range_i, range_j), so warps almost never diverge on it.
+//
+// Reciprocal square roots: FP32 uses rsqrt.approx.ftz.f32.  FP64 has no
+// full-precision hardware rsqrt; it is seeded with rsqrt.approx.ftz.f64 and
+// refined by one third-order Householder step for 1/sqrt
+// (y = y0 (1 + e/2 + 3 e^2 / 8), e = 1 - r2 y0^2), checked against
+// 1/sqrt(r2) to a few ulp by the test suite.
+#include "common.cuh"
+
+namespace sph {
+
+constexpr int kGThreads = 128;
+
+__device__ __forceinline__ float rsqrt_f32(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+__device__ __forceinline__ double rsqrt_f64(double x) {
+  double y0;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y0) : "d"(x));
+  const double e = fma(-x, y0 * y0, 1.0);
+  const double c = fma(0.375, e, 0.5);
+  return fma(y0 * e, c, y0);
+}
+
+// reference spline softening polynomials, sph_grav_kernel.cu:53-61
+template <class R>
+__device__ __forceinline__ void spline_poly(R u, R u2, R &gacc, R &gpot) {
+  const R u3 = u2 * u;
+  if (u < (R)0.5) {
+    gacc = (R)10.666666666667 + u2 * ((R)32.0 * u - (R)38.4);
+    gpot = (R)(-2.8) + u2 * ((R)5.333333333333 + u2 * ((R)6.4 * u - (R)9.6));
+  } else {
+    gacc = (R)21.333333333333 - (R)48.0 * u + (R)38.4 * u2 - (R)10.666666666667 * u3 - (R)0.066666666667 / u3;
+    gpot = (R)(-3.2) + (R)0.066666666667 / u + u2 * ((R)10.666666666667 + u * ((R)(-16.0) + u * ((R)9.6 - (R)2.133333333333 * u)));
+  }
+}
+
+template <class R>
+__device__ __forceinline__ R rsq(R x);
+template <>
+__device__ __forceinline__ float rsq<float>(float x) { return rsqrt_f32(x); }
+template <>
+__device__ __forceinline__ double rsq<double>(double x) { return rsqrt_f64(x); }
+
+// The near-field pair of the spline mode (r < max(range_i, range_j)),
+// bodyBodyInteraction's else-branch, sph_grav_kernel.cu:40-106.
+// dx = x_j - x_i; accumulates acceleration into a (a += contribution).
+template <class R>
+__device__ __noinline__ void spline_near(R dx, R dy, R dz, R r2, R mj, R hi2, R hj2, R &ax, R &ay, R &az, R &pot) {
+  R inv = r2 > 0 ? rsq<R>(r2) : (R)0;
+  R s3h = (R)0.5 * mj * inv * inv * inv;
+  R g;
+  if (r2 < hi2) {
+    const R u2 = r2 / hi2, h = sqrt(hi2), u = sqrt(u2);
+    R ga, gp;
+    spline_poly<R>(u, u2, ga, gp);
+    g = (R)0.5 * mj * ga / (hi2 * h);
+    pot += mj * gp / h;
+  } else {
+    g = s3h;
+    pot -= mj * inv;
+  }
+  if (r2 < hj2) {
+    const R u2 = r2 / hj2, h = sqrt(hj2), u = sqrt(u2);
+    R ga, gp;
+    spline_poly<R>(u, u2, ga, gp);
+    g += (R)0.5 * mj * ga / (hj2 * h);
+  } else {
+    g += s3h;
+  }
+  ax = fma(dx, g, ax);
+  ay = fma(dy, g, ay);
+  az = fma(dz, g, az);
+}
+
+// -------------------------------- FP64 --------------------------------------
+template <int SOFT, int R>
+__global__ void __launch_bounds__(kGThreads) k_grav_f64(int n, const double4 *__restrict__ src,
+                                                        const double *__restrict__ h2src, double4 *__restrict__ out,
+                                                        double eps2, double G) {
+  __shared__ double4 sj[kGThreads];
+  __shared__ double sh[SOFT == SPH_SOFT_SPLINE ? kGThreads : 1];
+  const int t = threadIdx.x;
+  const int i0 = blockIdx.x * kGThreads * R;
+  double xi[R], yi[R], zi[R], hi2[R], ax[R], ay[R], az[R], pot[R];
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    const int i = min(i0 + r * kGThreads + t, n - 1);
+    const double4 p = src[i];
+    xi[r] = p.x; yi[r] = p.y; zi[r] = p.z;
+    hi2[r] = (SOFT == SPH_SOFT_SPLINE) ? h2src[i] : 0.0;
+    ax[r] = ay[r] = az[r] = pot[r] = 0.0;
+  }
+  for (int j0 = 0; j0 < n; j0 += kGThreads) {
+    const int j = j0 + t;
+    __syncthreads();
+    if (j < n) {
+      sj[t] = src[j];
+      if (SOFT == SPH_SOFT_SPLINE) sh[t] = h2src[j];
+    }
+    __syncthreads();
+    const int m = min(kGThreads, n - j0);
+    if (SOFT == SPH_SOFT_PLUMMER) {
+#pragma unroll 4
+      for (int k = 0; k < m; k++) {
+        const double4 q = sj[k];
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+          const double dx = q.x - xi[r], dy = q.y - yi[r], dz = q.z - zi[r];
+          const double r2 = fma(dz, dz, fma(dy, dy, fma(dx, dx, eps2)));
+          const double inv = rsqrt_f64(r2);
+          const double s = q.w * inv;
+          const double s3 = s * inv * inv;
+          ax[r] = fma(dx, s3, ax[r]);
+          ay[r] = fma(dy, s3, ay[r]);
+          az[r] = fma(dz, s3, az[r]);
+          pot[r] -= s;
+        }
+      }
+    } else {
+      for (int k = 0; k < m; k++) {
+        const double4 q = sj[k];
+        const double hj2 = sh[k];
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+          const double dx = q.x - xi[r], dy = q.y - yi[r], dz = q.z - zi[r];
+          const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
+          if (r2 >= hi2[r] && r2 >= hj2) {
+            if (r2 > 0) {
+              const double inv = rsqrt_f64(r2);
+              const double s = q.w * inv;
+              const double s3 = s * inv * inv;
+              ax[r] = fma(dx, s3, ax[r]);
+              ay[r] = fma(dy, s3, ay[r]);
+              az[r] = fma(dz, s3, az[r]);
+              pot[r] -= s;
+            }
+          } else {
+            spline_near<double>(dx, dy, dz, r2, q.w, hi2[r], hj2, ax[r], ay[r], az[r], pot[r]);
+          }
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    const int i = i0 + r * kGThreads + t;
+    if (i < n) out[i] = make_double4(G * ax[r], G * ay[r], G * az[r], G * pot[r]);
+  }
+}
+
+// ----------------------------- mixed (FP32) ---------------------------------
+__device__ __forceinline__ void kahan_add(float &hi, float &lo, float v) {
+  // Knuth TwoSum of (hi, v); the rounding error joins lo
+  const float s = hi + v;
+  const float bp = s - hi;
+  const float err = (hi - (s - bp)) + (v - bp);
+  hi = s;
+  lo += err;
+}
+
+template <int SOFT, int R>
+__global__ void __launch_bounds__(kGThreads) k_grav_f32(int n, const double4 *__restrict__ src,
+                                                        const double *__restrict__ h2src, double4 *__restrict__ out,
+                                                        float eps2, double G) {
+  __shared__ float4 sj[kGThreads];
+  __shared__ float sh[SOFT == SPH_SOFT_SPLINE ? kGThreads : 1];
+  const int t = threadIdx.x;
+  const int i0 = blockIdx.x * kGThreads * R;
+  const double4 anc = src[min(i0, n - 1)];
+  float xi[R], yi[R], zi[R], hi2[R];
+  float ahi[R][4], alo[R][4];
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    const int i = min(i0 + r * kGThreads + t, n - 1);
+    const double4 p = src[i];
+    xi[r] = (float)(p.x - anc.x);
+    yi[r] = (float)(p.y - anc.y);
+    zi[r] = (float)(p.z - anc.z);
+    hi2[r] = (SOFT == SPH_SOFT_SPLINE) ? (float)h2src[i] : 0.f;
+#pragma unroll
+    for (int c = 0; c < 4; c++) ahi[r][c] = alo[r][c] = 0.f;
+  }
+  for (int j0 = 0; j0 < n; j0 += kGThreads) {
+    const int j = j0 + t;
+    __syncthreads();
+    if (j < n) {
+      const double4 q = src[j];
+      sj[t] = make_float4((float)(q.x - anc.x), (float)(q.y - anc.y), (float)(q.z - anc.z), (float)q.w);
+      if (SOFT == SPH_SOFT_SPLINE) sh[t] = (float)h2src[j];
+    }
+    __syncthreads();
+    const int m = min(kGThreads, n - j0);
+    float px[R], py[R], pz[R], pp[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) px[r] = py[r] = pz[r] = pp[r] = 0.f;
+    if (SOFT == SPH_SOFT_PLUMMER) {
+      if (m == kGThreads) {
+#pragma unroll 8
+        for (int k = 0; k < kGThreads; k++) {
+          const float4 q = sj[k];
+#pragma unroll
+          for (int r = 0; r < R; r++) {
+            const float dx = q.x - xi[r], dy = q.y - yi[r], dz = q.z - zi[r];
+            const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
+            const float inv = rsqrt_f32(r2);
+            const float s = q.w * inv;
+            const float s3 = s * inv * inv;
+            px[r] = fmaf(dx, s3, px[r]);
+            py[r] = fmaf(dy, s3, py[r]);
+            pz[r] = fmaf(dz, s3, pz[r]);
+            pp[r] -= s;
+          }
+        }
+      } else {
+        for (int k = 0; k < m; k++) {
+          const float4 q = sj[k];
+#pragma unroll
+          for (int r = 0; r < R; r++) {
+            const float dx = q.x - xi[r], dy = q.y - yi[r], dz = q.z - zi[r];
+            const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
+            const float inv = rsqrt_f32(r2);
+            const float s = q.w * inv;
+            const float s3 = s * inv * inv;
+            px[r] = fmaf(dx, s3, px[r]);
+            py[r] = fmaf(dy, s3, py[r]);
+            pz[r] = fmaf(dz, s3, pz[r]);
+            pp[r] -= s;
+          }
+        }
+      }
+    } else {
+      for (int k = 0; k < m; k++) {
+        const float4 q = sj[k];
+        const float hj2 = sh[k];
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+          const float dx = q.x - xi[r], dy = q.y - yi[r], dz = q.z - zi[r];
+          const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+          if (r2 >= hi2[r] && r2 >= hj2) {
+            if (r2 > 0) {
+              const float inv = rsqrt_f32(r2);
+              const float s = q.w * inv;
+              const float s3 = s * inv * inv;
+              px[r] = fmaf(dx, s3, px[r]);
+              py[r] = fmaf(dy, s3, py[r]);
+              pz[r] = fmaf(dz, s3, pz[r]);
+              pp[r] -= s;
+            }
+          } else {
+            spline_near<float>(dx, dy, dz, r2, q.w, hi2[r], hj2, px[r], py[r], pz[r], pp[r]);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      kahan_add(ahi[r][0], alo[r][0], px[r]);
+      kahan_add(ahi[r][1], alo[r][1], py[r]);
+      kahan_add(ahi[r][2], alo[r][2], pz[r]);
+      kahan_add(ahi[r][3], alo[r][3], pp[r]);
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    const int i = i0 + r * kGThreads + t;
+    if (i < n)
+      out[i] = make_double4(G * ((double)ahi[r][0] + (double)alo[r][0]), G * ((double)ahi[r][1] + (double)alo[r][1]),
+                            G * ((double)ahi[r][2] + (double)alo[r][2]), G * ((double)ahi[r][3] + (double)alo[r][3]));
+  }
+}
+
+// src = {x, y, z, m} per particle; h2src = range^2 (spline mode only)
+int launch_gravity(int n, const double4 *src, const double *h2src, double4 *out, int soft_mode, double eps, double G,
+                   int precision, cudaStream_t st) {
+  if (n <= 0) return 0;
+  const double eps2 = eps * eps;
+  if (precision == SPH_PREC_FP64) {
+    constexpr int R = 2;
+    const int blocks = (n + kGThreads * R - 1) / (kGThreads * R);
+    if (soft_mode == SPH_SOFT_PLUMMER)
+      k_grav_f64<SPH_SOFT_PLUMMER, R><<<blocks, kGThreads, 0, st>>>(n, src, h2src, out, eps2, G);
+    else
+      k_grav_f64<SPH_SOFT_SPLINE, R><<<blocks, kGThreads, 0, st>>>(n, src, h2src, out, eps2, G);
+  } else {
+    constexpr int R = 4;
+    const int blocks = (n + kGThreads * R - 1) / (kGThreads * R);
+    if (soft_mode == SPH_SOFT_PLUMMER)
+      k_grav_f32<SPH_SOFT_PLUMMER, R><<<blocks, kGThreads, 0, st>>>(n, src, h2src, out, (float)eps2, G);
+    else
+      k_grav_f32<SPH_SOFT_SPLINE, R><<<blocks, kGThreads, 0, st>>>(n, src, h2src, out, (float)eps2, G);
+  }
+  return 1;
+}
+
+// pack the gravity sources {x, y, z, m} and range^2 from the state
+__global__ void k_pack_sources(int n, const double4 *__restrict__ pos, const double4 *__restrict__ vel,
+                               double4 *__restrict__ src, double *__restrict__ h2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double4 p = pos[i];
+  src[i] = make_double4(p.x, p.y, p.z, vel[i].w);
+  h2[i] = p.w * p.w;
+}
+
+int launch_pack_sources(int n, const double4 *pos, const double4 *vel, double4 *src, double *h2, cudaStream_t st) {
+  k_pack_sources<<<(n + 255) / 256, 256, 0, st>>>(n, pos, vel, src, h2);
+  return 1;
+}
+
+__global__ void k_range_sq(int n, const double *__restrict__ r, double *__restrict__ h2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) h2[i] = r ? r[i] * r[i] : 0.0;
+}
+
+}  // namespace sph
+
+extern "C" int cudasph_gravity_direct(int n, const double *pos4, const double *range, double *out4, int soft_mode,
+                                      double eps, double G, int precision, void *stream) {
+  if (n < 0 || (n > 0 && (!pos4 || !out4))) return SPH_ERR_ARG;
+  if (soft_mode == SPH_SOFT_PLUMMER && !(eps > 0)) return SPH_ERR_ARG;
+  if (soft_mode == SPH_SOFT_SPLINE && !range) return SPH_ERR_ARG;
+  if (n == 0) return SPH_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  double *h2 = nullptr;
+  if (soft_mode == SPH_SOFT_SPLINE) {
+    SPH_CUDA_TRY(cudaMallocAsync((void **)&h2, sizeof(double) * n, st));
+    sph::k_range_sq<<<(n + 255) / 256, 256, 0, st>>>(n, range, h2);
+  }
+  sph::launch_gravity(n, (const double4 *)pos4, h2, (double4 *)out4, soft_mode, eps, G, precision, st);
+  if (h2) SPH_CUDA_TRY(cudaFreeAsync(h2, st));
+  SPH_CUDA_TRY(cudaGetLastError());
+  return SPH_OK;
+}

@@ -1,0 +1,249 @@
+// hydro.cu -- FP64 density loop (dev_density_loop.cu:29-111), EOS
+// (dev_compute_pressure.cu:3-111), hydro derivatives with Monaghan artificial
+// viscosity (dev_hydro_dots.cu:25-113, dev_art_visc.cu:8-32) and the j-side
+// pair force (add_ngb_acc, sph_accelerations.cpp:106-114).
+//
+// One warp per leaf, one lane per particle.  The neighbour list of lane l is
+// read from the leaf-sliced layout, so entry k of all 32 lanes is one
+// coalesced 128-byte load; neighbour records (double4 pos / vel / hydro /
+// dots_data) are gathered with 16-byte loads and mostly hit L1/L2 because
+// neighbours are Morton-close.  The j-side force of each pair is added to
+// the neighbour with an FP64 atomic (red.global.add.f64), which keeps the
+// pair force antisymmetric (momentum conserving) without a transposed list.
+//
+// Compiled without FMA contraction, like neighbours.cu: the per-particle sums
+// follow the operation order of an FP64 CPU evaluation of the same loops.
+#include "common.cuh"
+#include "sph_math.cuh"
+
+namespace sph {
+
+
+__device__ __forceinline__ int leaf_max_count(int cnt) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) cnt = max(cnt, __shfl_xor_sync(0xffffffffu, cnt, o));
+  return cnt;
+}
+
+__global__ void __launch_bounds__(128) k_density(HydroArgs a) {
+  const int leaf = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (leaf >= a.nleaf) return;
+  const int lane = (int)lane_id();
+  const int s = leaf * kLeaf + lane;
+  const bool valid = s < a.n;
+  double4 pi = make_double4(0, 0, 0, 0), vi = make_double4(0, 0, 0, 0);
+  int cnt = 0;
+  if (valid) {
+    pi = a.pos[s];
+    vi = a.vel[s];
+    cnt = min(a.n_ngb[s], a.cap);
+  }
+  const int kmax = leaf_max_count(cnt);
+  const int *lst = a.list + (size_t)leaf * a.cap * kLeaf + lane;
+  const double w = pi.w;
+  double dens = 0, om = 0, ps = 0, sdig = 0, div = 0, cx = 0, cy = 0, cz = 0;
+  for (int k = 0; k < kmax; k++) {
+    if (k < cnt) {
+      const int j = __ldg(lst + (size_t)k * kLeaf);
+      const double4 pj = ld4(a.pos + j), vj = ld4(a.vel + j);
+      const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+      const double u = 2 * sqrt(ds2_exact(dx, dy, dz)) / w;
+      const double mj = vj.w;
+      dens += mj * k_w<double>(u);
+      om += mj * k_dwdh<double>(u);
+      ps += mj * k_dphidh<double>(u);
+      sdig -= k_digdh<double>(u);
+      const double dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
+      const double wt = mj * k_dw<double>(u);
+      div += wt * (dx * dvx + dy * dvy + dz * dvz);
+      cx += wt * (dy * dvz - dz * dvy);
+      cy += wt * (dz * dvx - dx * dvz);
+      cz += wt * (dx * dvy - dy * dvx);
+    }
+  }
+  if (!valid) return;
+  double4 d = make_double4(0, 0, 0, 0);
+  double rho = 0;
+  if (w > 0 && cnt > 0) {
+    const double h = 0.5 * w;
+    const double h3 = h * h * h, h5 = h3 * h * h;
+    if (sdig != 0) {
+      om *= 1.0 / h3 / sdig;
+      ps *= 1.0 / h / sdig;
+    } else {
+      om = ps = 0;
+    }
+    dens *= 1.0 / h3;
+    div *= 1.0 / dens / h5;
+    const double c = sqrt(cx * cx + cy * cy + cz * cz) / dens / h5;
+    rho = dens;
+    d = make_double4(div, c, om, ps);
+  }
+  a.hyd[s].x = rho;
+  a.dd[s] = d;
+}
+
+// ---------------------------------------------------------------------------
+// EOS.  The temperature solves u = u_gas(T) + u_rad(T), i.e. the quartic
+// x^4 + q x + r = 0 in x = T / 1e6 (dev_compute_pressure.cu:83-96): the
+// closed form of dev_compute_pressure.cu:3-49 (resolvent cubic), then Newton
+// polish in FP64 from the nearer of the closed form and the upper bound
+// min(-r/q, (-r)^(1/4)).
+// ---------------------------------------------------------------------------
+constexpr double kDensityUnit = 5.89994031541978;     // dev_compute_pressure.cu:57-58
+constexpr double kEnergyUnit = 1.90698842928778e+15;  // :61-62
+constexpr double kPressureUnit = 1.1251117914994e+16; // :65-66
+constexpr double kAmu = 1.66054e-24;                   // :69-70
+constexpr double kBoltzmann = 1.380658e-16;            // :73-74
+constexpr double kRadConst = 7.56591414984829e-15;     // :77-78
+
+__device__ double quartic_root(double q, double r) {
+  const double kh = 0.5 * 0.125 * q * q;
+  const double disc = kh * kh - r * r * r / 27.0;
+  const double sd = sqrt(disc);
+  const double p1 = kh + sd, p2 = kh - sd;
+  const double y = cbrt(p1) - cbrt(fabs(p2));
+  const double b2 = sqrt(2.0 * y);
+  const double c2 = y - 0.5 * q / b2;
+  double x = 0.5 * (sqrt(b2 * b2 - 4 * c2) - b2);
+  if (p1 == -p2) x = pow(-r - q * pow(-r - q * pow(-r, 0.25), 0.25), 0.25);
+  if (p2 > 0) x = -(r + r * r * r * r / (q * q * q * q)) / q;
+  double ub = -r / q;
+  const double ub2 = pow(-r, 0.25);
+  if (ub2 < ub) ub = ub2;
+  if (!(x > 0) || !(x <= ub) || !isfinite(x)) x = ub;
+  for (int it = 0; it < 8; it++) {
+    const double x3 = x * x * x;
+    const double f = x3 * x + q * x + r;
+    const double fp = 4 * x3 + q;
+    double xn = x - f / fp;
+    if (!(xn > 0)) xn = 0.5 * x;
+    if (xn == x) break;
+    x = xn;
+  }
+  return x;
+}
+
+__device__ __forceinline__ double pressure_of(double rho, double u, double mu, int eos_mode, double gamma) {
+  if (eos_mode == SPH_EOS_IDEAL) return (gamma - 1) * rho * u;
+  if (!(rho > 0) || !(mu > 0)) return 0;
+  const double density = rho * kDensityUnit;
+  const double energy = u * kEnergyUnit;
+  const double mean_mu = mu * kAmu;
+  const double tb = 1.0e6;
+  const double r = -density * (energy / (tb * tb)) / (kRadConst * tb * tb);
+  const double q = (kBoltzmann / kRadConst) / (gamma - 1) * density / (((mean_mu * tb) * tb) * tb);
+  const double T = tb * quartic_root(q, r);
+  const double pg = density * ((kBoltzmann * T) / mean_mu);
+  const double pr = (((kRadConst / 3.0 * T) * T) * T) * T;
+  return (pg + pr) / kPressureUnit;
+}
+
+__global__ void k_pressure(int n, double4 *__restrict__ hyd, int eos_mode, double gamma, unsigned *flags) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double4 h = hyd[i];
+  const double P = pressure_of(h.x, h.z, h.w, eos_mode, gamma);
+  if (!isfinite(P)) raise_flag(flags, SPH_FLAG_NONFINITE);
+  hyd[i].y = P;
+}
+
+// dev_art_visc.cu:8-32 in FP64
+__device__ __forceinline__ void art_visc(double range_i, double range_j, double ds, double drdv, double rho_i,
+                                         double P_i, double div_i, double curl_i, double rho_j, double P_j,
+                                         double div_j, double curl_j, double alpha, double beta, double gamma,
+                                         double &visc, double &vsig) {
+  double ci = sqrt(gamma * P_i / rho_i);
+  double cj = sqrt(gamma * P_j / rho_j);
+  double av = 0, vs = ci + cj;
+  if (drdv < 0) {
+    vs -= beta * drdv / ds;
+    av = drdv / ((ci + cj) * ds);
+    const double bi = fabs(div_i) / (fabs(div_i) + curl_i + 0.0001 * ci / (0.5 * range_i));
+    const double bj = fabs(div_j) / (fabs(div_j) + curl_j + 0.0001 * cj / (0.5 * range_j));
+    av *= (bi + bj);
+    av = (P_i / (rho_i * rho_i) + P_j / (rho_j * rho_j)) * (-alpha * av + beta * av * av);
+  }
+  visc = av;
+  vsig = vs;
+}
+
+// hydro_dots (dev_hydro_dots.cu:25-113) plus the j-side of every pair.
+// dots must be zero on entry (xyz accumulate); dots.w (du/dt) is stored.
+__global__ void __launch_bounds__(128) k_hydro(HydroArgs a) {
+  const int leaf = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (leaf >= a.nleaf) return;
+  const int lane = (int)lane_id();
+  const int s = leaf * kLeaf + lane;
+  const bool valid = s < a.n;
+  double4 pi = make_double4(0, 0, 0, 0), vi = make_double4(0, 0, 0, 1), hi4 = make_double4(0, 0, 0, 0),
+          di = make_double4(0, 0, 0, 0);
+  int cnt = 0;
+  if (valid) {
+    pi = a.pos[s];
+    vi = a.vel[s];
+    hi4 = a.hyd[s];
+    di = a.dd[s];
+    cnt = min(a.n_ngb[s], a.cap);
+  }
+  const int kmax = leaf_max_count(cnt);
+  const int *lst = a.list + (size_t)leaf * a.cap * kLeaf + lane;
+  const double hh = 0.5 * pi.w;
+  const double prho2 = (hi4.x > 0) ? hi4.y / (hi4.x * hi4.x) : 0;
+  const double h2 = hh * hh, h5 = h2 * h2 * hh;
+  const double psi_i = a.use_psi ? di.w : 0;
+  double axi = 0, ayi = 0, azi = 0, udot = 0, vmax = 0;
+  for (int k = 0; k < kmax; k++) {
+    if (k < cnt) {
+      const int j = __ldg(lst + (size_t)k * kLeaf);
+      const double4 pj = ld4(a.pos + j), vj = ld4(a.vel + j), hj = ld4(a.hyd + j), dj = ld4(a.dd + j);
+      const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+      const double dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
+      const double ds = sqrt(ds2_exact(dx, dy, dz));
+      const double u = ds / hh;
+      const double drdv = dx * dvx + dy * dvy + dz * dvz;
+      double visc, vs;
+      art_visc(pi.w, pj.w, ds, drdv, hi4.x, hi4.y, di.x, di.y, hj.x, hj.y, dj.x, dj.y, a.alpha, a.beta, a.gamma,
+               visc, vs);
+      if (vs > vmax) vmax = vs;
+      const double dwu = k_dw<double>(u), digu = k_dig<double>(u);
+      const double mj = vj.w;
+      double acc = (prho2 + 0.5 * visc) * dwu / h5;
+      acc -= (prho2 * di.z + 0.5 * psi_i) / mj * digu / h2;
+      axi -= mj * acc * dx;
+      ayi -= mj * acc * dy;
+      azi -= mj * acc * dz;
+      const double nacc = vi.w * acc;
+      if (a.ngb_acc) a.ngb_acc[(size_t)leaf * a.cap * kLeaf + (size_t)k * kLeaf + lane] = nacc;
+      if (a.jside && j != s) {
+        atomicAdd(&a.dots[j].x, nacc * dx);
+        atomicAdd(&a.dots[j].y, nacc * dy);
+        atomicAdd(&a.dots[j].z, nacc * dz);
+      }
+      double ud = mj * (prho2 + 0.5 * visc) * dwu / h5;
+      ud -= prho2 * di.z * digu / h2;
+      udot += ud * drdv;
+    }
+  }
+  if (!valid) return;
+  atomicAdd(&a.dots[s].x, axi);
+  atomicAdd(&a.dots[s].y, ayi);
+  atomicAdd(&a.dots[s].z, azi);
+  a.dots[s].w = udot;
+  a.vsig[s] = vmax;
+}
+
+int launch_density(const HydroArgs &a, cudaStream_t st) {
+  k_density<<<(a.nleaf * 32 + 127) / 128, 128, 0, st>>>(a);
+  return 1;
+}
+int launch_pressure(int n, double4 *hyd, int eos_mode, double gamma, unsigned *flags, cudaStream_t st) {
+  k_pressure<<<(n + 255) / 256, 256, 0, st>>>(n, hyd, eos_mode, gamma, flags);
+  return 1;
+}
+int launch_hydro(const HydroArgs &a, cudaStream_t st) {
+  k_hydro<<<(a.nleaf * 32 + 127) / 128, 128, 0, st>>>(a);
+  return 1;
+}
+
+}  // namespace sph

@@ -1,0 +1,308 @@
+// neighbours.cu -- smoothing-length solve (dev_solve_range.cu:17-189) and
+// neighbour search (dev_find_ngb.cu:13-87) on the Morton tree.
+//
+// One warp owns one leaf (32 consecutive particles); lane l owns particle
+// 32*leaf + l.  The warp walks the tree together: at every internal node each
+// lane tests one child box, a ballot picks the children that overlap the
+// union of the lanes' search boxes, and the hits are pushed in reverse order
+// on a per-warp shared-memory stack, so leaves come out in ascending index
+// order.  A visited leaf's 32 positions are staged in shared memory and every
+// lane applies the exact FP64 predicate ds2 < range^2 to all of them.
+//
+// This translation unit is compiled without FMA contraction: the h solve and
+// the predicate then perform the same IEEE operations, in the same order
+// (ascending neighbour index), as an FP64 CPU evaluation of the reference's
+// loops, which makes the solved ranges and the neighbour sets reproducible
+// bit for bit against such an evaluation.
+#include "common.cuh"
+#include "sph_math.cuh"
+
+namespace sph {
+
+constexpr int kWarpsPerBlock = 4;
+constexpr unsigned kFull = 0xffffffffu;
+
+struct WarpSmem {
+  int stack[kStack];
+  double sx[kLeaf], sy[kLeaf], sz[kLeaf];
+};
+
+// Query box over the lanes that take part: [x - r, x + r] widened by a
+// relative 1e-15 of the magnitudes (covers the rounding of x - r) and
+// rounded outward to float.
+__device__ __forceinline__ void warp_query_box(bool on, double x, double y, double z, double r, float *ql, float *qh) {
+  double m0 = (fabs(x) + r) * 1e-15, m1 = (fabs(y) + r) * 1e-15, m2 = (fabs(z) + r) * 1e-15;
+  double l0 = on ? x - r - m0 : 1e308, l1 = on ? y - r - m1 : 1e308, l2 = on ? z - r - m2 : 1e308;
+  double h0 = on ? x + r + m0 : -1e308, h1 = on ? y + r + m1 : -1e308, h2 = on ? z + r + m2 : -1e308;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    l0 = fmin(l0, __shfl_xor_sync(kFull, l0, o));
+    l1 = fmin(l1, __shfl_xor_sync(kFull, l1, o));
+    l2 = fmin(l2, __shfl_xor_sync(kFull, l2, o));
+    h0 = fmax(h0, __shfl_xor_sync(kFull, h0, o));
+    h1 = fmax(h1, __shfl_xor_sync(kFull, h1, o));
+    h2 = fmax(h2, __shfl_xor_sync(kFull, h2, o));
+  }
+  ql[0] = __double2float_rd(l0); ql[1] = __double2float_rd(l1); ql[2] = __double2float_rd(l2);
+  qh[0] = __double2float_ru(h0); qh[1] = __double2float_ru(h1); qh[2] = __double2float_ru(h2);
+}
+
+// Visit, in ascending order, every leaf whose box overlaps [ql, qh].  All
+// lanes call visit(leaf) together.  Returns false on stack overflow.
+template <class Visit>
+__device__ bool walk_leaves(const TreeView &t, const float *ql, const float *qh, int *stack, Visit &&visit) {
+  const unsigned lane = lane_id();
+  const int top = t.levels - 1;
+  if (top == 0) {
+    visit(0);
+    return true;
+  }
+  int sp = 1;
+  if (lane == 0) stack[0] = (top << 26);
+  __syncwarp();
+  while (sp > 0) {
+    --sp;
+    const int e = stack[sp];
+    __syncwarp();
+    const int level = e >> 26, node = e & ((1 << 26) - 1);
+    const int cl = level - 1;
+    const int child = node * kFan + (int)lane;
+    bool hit = false;
+    if (child < t.count[cl]) {
+      const float4 l = __ldg(&t.lo[t.base[cl] + child]);
+      const float4 h = __ldg(&t.hi[t.base[cl] + child]);
+      hit = (l.x <= qh[0]) & (h.x >= ql[0]) & (l.y <= qh[1]) & (h.y >= ql[1]) & (l.z <= qh[2]) & (h.z >= ql[2]);
+    }
+    unsigned m = __ballot_sync(kFull, hit);
+    if (cl == 0) {
+      while (m) {
+        const int b = __ffs(m) - 1;
+        m &= m - 1;
+        visit(node * kFan + b);
+      }
+      continue;
+    }
+    const int cnt = __popc(m);
+    if (sp + cnt > kStack) return false;
+    if (hit) stack[sp + cnt - 1 - __popc(m & ((1u << lane) - 1u))] = (cl << 26) | child;
+    sp += cnt;
+    __syncwarp();
+  }
+  return true;
+}
+
+__device__ __forceinline__ void stage_leaf(const double4 *__restrict__ pos, int n, int leaf, WarpSmem &sm) {
+  const int s = leaf * kLeaf + (int)lane_id();
+  __syncwarp();
+  if (s < n) {
+    const double4 p = ld4(pos + s);
+    sm.sx[lane_id()] = p.x;
+    sm.sy[lane_id()] = p.y;
+    sm.sz[lane_id()] = p.z;
+  }
+  __syncwarp();
+}
+
+struct SolveArgs {
+  TreeView t;
+  double4 *pos;
+  int *nevals;
+  unsigned *flags;
+  double n_target, rel_err, f_scale;
+  int max_iter;
+};
+
+enum { kBr0 = 0, kBr1 = 1, kSolve = 2, kDone = 3 };
+
+// dev_solve_range (dev_solve_range.cu:137-189): per particle, bracket the
+// root of f(w) = sum_j ig(2 r_ij / w) - N_target with clamped Newton steps
+// (dev_bracket_root :93-135), then safeguarded Newton / bisection until
+// |dx| < rel_err * w.  Each lane runs that iteration as a state machine; the
+// lanes that need an evaluation of f in a round share one tree walk.
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) k_solve_range(SolveArgs a) {
+  __shared__ WarpSmem smem[kWarpsPerBlock];
+  WarpSmem &sm = smem[threadIdx.x >> 5];
+  const int leaf = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int n = a.t.n;
+  if (leaf >= a.t.count[0]) return;
+  const int s = leaf * kLeaf + (int)lane_id();
+  const bool valid = s < n;
+  double xi = 0, yi = 0, zi = 0, w = 0;
+  if (valid) {
+    const double4 p = a.pos[s];
+    xi = p.x; yi = p.y; zi = p.z; w = p.w;
+  }
+  int phase = (valid && w > 0) ? kBr0 : kDone;
+  double dx = 0, f = 0, x_left = 0, f_try = 0, rx = 0, ry = 0;
+  int iter = 0, keep = 0, nev = 0;
+  bool stack_ok = true;
+  const double rel = a.rel_err, fs = a.f_scale;
+  while (true) {
+    const bool need = phase != kDone;
+    if (!__any_sync(kFull, need)) break;
+    float ql[3], qh[3];
+    warp_query_box(need, xi, yi, zi, w, ql, qh);
+    double sf = 0, sg = 0, sc = 0;
+    const double w2 = __dmul_rn(w, w);
+    stack_ok &= walk_leaves(a.t, ql, qh, sm.stack, [&](int lj) {
+      stage_leaf(a.pos, n, lj, sm);
+      const int cnt = min(kLeaf, n - lj * kLeaf);
+      if (need) {
+        for (int k = 0; k < cnt; k++) {
+          const double d2 = ds2_exact(xi - sm.sx[k], yi - sm.sy[k], zi - sm.sz[k]);
+          if (d2 < w2) {
+            const double u = 2 * sqrt(d2) / w;
+            sf += k_ig<double>(u);
+            sg -= k_digdh<double>(u);
+            sc += 1;
+          }
+        }
+      }
+    });
+    if (!need) continue;
+    nev++;
+    // compute_ngb epilogue, dev_solve_range.cu:77-87
+    f = sf - a.n_target;
+    sg *= 1.0 / w;
+    if (sg != 0) dx = f / sg;
+    else dx = (f < 0) ? -w : +w;
+    // advance this lane's iteration to its next evaluation (or the end)
+    bool to_solve_init = false, to_br_check = false, to_solve_check = false;
+    if (phase == kBr0 || phase == kBr1) {
+      if (fabs(dx) < rel * w) {
+        rx = w - 0.5 * fabs(dx);
+        ry = w + 0.5 * fabs(dx);
+        to_solve_init = true;
+      } else {
+        if (fabs(dx) > fs * w) dx = (dx < 0) ? -fs * w : fs * w;
+        if (phase == kBr0) {
+          x_left = w;
+          f_try = f;
+          iter = 0;
+        }
+        to_br_check = true;
+      }
+    } else {  // kSolve
+      if (f < 0) rx = w;
+      else ry = w;
+      keep = fabs(dx) > rel * w;
+      to_solve_check = true;
+    }
+    if (to_br_check) {
+      if ((f_try * f >= 0) && (iter++ < a.max_iter)) {
+        x_left = w;
+        f_try = f;
+        w -= dx;
+        phase = kBr1;
+      } else {
+        if (x_left < w) { rx = x_left; ry = w; }
+        else { rx = w; ry = x_left; }
+        to_solve_init = true;
+      }
+    }
+    if (to_solve_init) {
+      w = 0.5 * (rx + ry);
+      dx = 0;
+      if (fabs(rx - ry) > rel * w) {
+        iter = 0;
+        keep = 1;
+        to_solve_check = true;
+      } else {
+        phase = kDone;
+      }
+    }
+    if (to_solve_check) {
+      if (keep && (iter++ < a.max_iter)) {
+        w -= dx;
+        if ((w - ry) * (w - rx) >= 0) {
+          dx = 0.5 * (ry - rx);
+          w = 0.5 * (rx + ry);
+        }
+        phase = kSolve;
+      } else {
+        if (keep) raise_flag(a.flags, SPH_FLAG_H_NOT_CONVERGED);
+        phase = kDone;
+      }
+    }
+  }
+  if (!stack_ok && lane_id() == 0) raise_flag(a.flags, SPH_FLAG_STACK_OVERFLOW);
+  if (valid) {
+    a.pos[s].w = (w > 0) ? w : 0.0;
+    if (a.nevals) a.nevals[s] = nev;
+  }
+}
+
+struct FindArgs {
+  TreeView t;
+  const double4 *pos;
+  int *n_ngb;
+  int *list;       // [leaf][k][lane], cap entries per lane
+  int cap;
+  unsigned *flags;
+};
+
+// dev_find_ngb (dev_find_ngb.cu:13-87): every j with ds2 < range_i^2, in
+// ascending slot order, written to the leaf-sliced list (entry k of lane l of
+// leaf L at ((L * cap) + k) * 32 + l: the lanes of a warp read and write
+// their k-th neighbours in one 128-byte transaction).
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) k_find_ngb(FindArgs a) {
+  __shared__ WarpSmem smem[kWarpsPerBlock];
+  WarpSmem &sm = smem[threadIdx.x >> 5];
+  const int leaf = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int n = a.t.n;
+  if (leaf >= a.t.count[0]) return;
+  const int s = leaf * kLeaf + (int)lane_id();
+  const bool valid = s < n;
+  double xi = 0, yi = 0, zi = 0, w = 0;
+  if (valid) {
+    const double4 p = a.pos[s];
+    xi = p.x; yi = p.y; zi = p.z; w = p.w;
+  }
+  const bool on = valid && w > 0;
+  float ql[3], qh[3];
+  warp_query_box(on, xi, yi, zi, w, ql, qh);
+  const double w2 = __dmul_rn(w, w);
+  int cnt = 0;
+  int *out = a.list + (size_t)leaf * a.cap * kLeaf + lane_id();
+  const int cap = a.cap;
+  bool ok = true;
+  if (__any_sync(kFull, on)) {
+    ok = walk_leaves(a.t, ql, qh, sm.stack, [&](int lj) {
+      stage_leaf(a.pos, n, lj, sm);
+      const int m = min(kLeaf, n - lj * kLeaf);
+      if (on) {
+        for (int k = 0; k < m; k++) {
+          const double d2 = ds2_exact(xi - sm.sx[k], yi - sm.sy[k], zi - sm.sz[k]);
+          if (d2 < w2) {
+            if (cnt < cap) out[(size_t)cnt * kLeaf] = lj * kLeaf + k;
+            cnt++;
+          }
+        }
+      }
+    });
+  }
+  if (!ok && lane_id() == 0) raise_flag(a.flags, SPH_FLAG_STACK_OVERFLOW);
+  if (cnt > cap) raise_flag(a.flags, SPH_FLAG_NGB_OVERFLOW);
+  if (valid) a.n_ngb[s] = cnt;
+}
+
+int launch_solve_range(const TreeView &t, double4 *pos, int *nevals, unsigned *flags, const sph_params &p,
+                       cudaStream_t st) {
+  SolveArgs a;
+  a.t = t; a.pos = pos; a.nevals = nevals; a.flags = flags;
+  a.n_target = p.n_target; a.rel_err = p.rel_err; a.f_scale = p.f_scale; a.max_iter = p.max_iter;
+  const int warps = t.count[0];
+  k_solve_range<<<(warps + kWarpsPerBlock - 1) / kWarpsPerBlock, kWarpsPerBlock * 32, 0, st>>>(a);
+  return 1;
+}
+
+int launch_find_ngb(const TreeView &t, const double4 *pos, int *n_ngb, int *list, int cap, unsigned *flags,
+                    cudaStream_t st) {
+  FindArgs a;
+  a.t = t; a.pos = pos; a.n_ngb = n_ngb; a.list = list; a.cap = cap; a.flags = flags;
+  const int warps = t.count[0];
+  k_find_ngb<<<(warps + kWarpsPerBlock - 1) / kWarpsPerBlock, kWarpsPerBlock * 32, 0, st>>>(a);
+  return 1;
+}
+
+}  // namespace sph

@@ -1,0 +1,244 @@
+// sort.cu -- Morton keys and a stable LSD radix sort (the space-filling-curve
+// sort of sort_bodies.cpp:119-186, done on the device every step).
+//
+// Keys: positions quantised to 21 bits per dimension in the bounding cube
+// (scale = 2^21 / max extent, like domain_fac of sort_bodies.cpp:135), bits
+// interleaved x-y-z from the top.  The sort is an 8-bit-digit LSD radix sort
+// (8 passes over 64-bit keys): per pass a per-block digit histogram, one
+// exclusive scan over [digit][block], and a stable scatter in which each
+// warp ranks equal digits with __match_any_sync.  Ties keep their input
+// order, so with values = slot indices the permutation equals a stable sort.
+#include <cub/block/block_scan.cuh>
+
+#include "common.cuh"
+
+namespace sph {
+
+constexpr int kRadixThreads = 256;
+constexpr int kRadixChunk = 4096;  // keys per block per pass
+
+__global__ void k_bbox_partial(int n, const double4 *__restrict__ pos, const double *__restrict__ x,
+                               const double *__restrict__ y, const double *__restrict__ z, double *__restrict__ part) {
+  double lo[3] = {1e308, 1e308, 1e308}, hi[3] = {-1e308, -1e308, -1e308};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double c[3];
+    if (pos) {
+      double4 p = pos[i];
+      c[0] = p.x; c[1] = p.y; c[2] = p.z;
+    } else {
+      c[0] = x[i]; c[1] = y[i]; c[2] = z[i];
+    }
+#pragma unroll
+    for (int d = 0; d < 3; d++) { lo[d] = fmin(lo[d], c[d]); hi[d] = fmax(hi[d], c[d]); }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      lo[d] = fmin(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+      hi[d] = fmax(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+    }
+  __shared__ double s[32][6];
+  int w = threadIdx.x >> 5;
+  if (lane_id() == 0)
+    for (int d = 0; d < 3; d++) { s[w][d] = lo[d]; s[w][3 + d] = hi[d]; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int nw = blockDim.x >> 5;
+    for (int k = 1; k < nw; k++)
+      for (int d = 0; d < 3; d++) { s[0][d] = fmin(s[0][d], s[k][d]); s[0][3 + d] = fmax(s[0][3 + d], s[k][3 + d]); }
+    for (int d = 0; d < 6; d++) part[blockIdx.x * 6 + d] = s[0][d];
+  }
+}
+
+// box4 = {lo.x, lo.y, lo.z, scale}; scale = 2^21 / max extent (0 if degenerate)
+__global__ void k_bbox_final(int nb, const double *__restrict__ part, double *__restrict__ box4) {
+  if (threadIdx.x != 0) return;
+  double lo[3] = {1e308, 1e308, 1e308}, hi[3] = {-1e308, -1e308, -1e308};
+  for (int b = 0; b < nb; b++)
+    for (int d = 0; d < 3; d++) { lo[d] = fmin(lo[d], part[b * 6 + d]); hi[d] = fmax(hi[d], part[b * 6 + 3 + d]); }
+  double size = hi[0] - lo[0];
+  if (hi[1] - lo[1] > size) size = hi[1] - lo[1];
+  if (hi[2] - lo[2] > size) size = hi[2] - lo[2];
+  box4[0] = lo[0]; box4[1] = lo[1]; box4[2] = lo[2];
+  box4[3] = size > 0 ? __ddiv_rn(2097152.0, size) : 0.0;
+}
+
+__device__ __forceinline__ uint64_t spread3(uint32_t v) {
+  uint64_t x = v & 0x1fffffu;
+  x = (x | (x << 32)) & 0x1f00000000ffffULL;
+  x = (x | (x << 16)) & 0x1f0000ff0000ffULL;
+  x = (x | (x << 8)) & 0x100f00f00f00f00fULL;
+  x = (x | (x << 4)) & 0x10c30c30c30c30c3ULL;
+  x = (x | (x << 2)) & 0x1249249249249249ULL;
+  return x;
+}
+
+__device__ __forceinline__ uint32_t quant21(double c, double lo, double scale) {
+  double v = __dmul_rn(__dsub_rn(c, lo), scale);
+  return v >= 2097151.0 ? 2097151u : (uint32_t)v;
+}
+
+__global__ void k_morton(int n, const double4 *__restrict__ pos, const double *__restrict__ x,
+                         const double *__restrict__ y, const double *__restrict__ z, const double *__restrict__ box4,
+                         uint64_t *__restrict__ keys, uint32_t *__restrict__ vals) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double c0, c1, c2;
+  if (pos) {
+    double4 p = pos[i];
+    c0 = p.x; c1 = p.y; c2 = p.z;
+  } else {
+    c0 = x[i]; c1 = y[i]; c2 = z[i];
+  }
+  double s = box4[3];
+  uint32_t qx = quant21(c0, box4[0], s), qy = quant21(c1, box4[1], s), qz = quant21(c2, box4[2], s);
+  keys[i] = (spread3(qx) << 2) | (spread3(qy) << 1) | spread3(qz);
+  if (vals) vals[i] = (uint32_t)i;
+}
+
+// per-block digit histogram, stored digit-major: hist[d * nb + block]
+__global__ void __launch_bounds__(kRadixThreads) k_radix_hist(int n, const uint64_t *__restrict__ keys, int shift,
+                                                              unsigned *__restrict__ hist) {
+  __shared__ unsigned h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  int beg = blockIdx.x * kRadixChunk, end = min(n, beg + kRadixChunk);
+  for (int i = beg + threadIdx.x; i < end; i += kRadixThreads) atomicAdd(&h[(keys[i] >> shift) & 255u], 1u);
+  __syncthreads();
+  hist[threadIdx.x * gridDim.x + blockIdx.x] = h[threadIdx.x];
+}
+
+// exclusive scan of m entries in one block of 1024 threads
+__global__ void __launch_bounds__(1024) k_radix_scan(int m, unsigned *__restrict__ hist) {
+  typedef cub::BlockScan<unsigned, 1024> Scan;
+  __shared__ typename Scan::TempStorage tmp;
+  int per = (m + 1023) / 1024;
+  int beg = threadIdx.x * per, end = min(m, beg + per);
+  unsigned s = 0;
+  for (int i = beg; i < end; i++) s += hist[i];
+  unsigned pre;
+  Scan(tmp).ExclusiveSum(s, pre);
+  for (int i = beg; i < end; i++) {
+    unsigned v = hist[i];
+    hist[i] = pre;
+    pre += v;
+  }
+}
+
+__global__ void __launch_bounds__(kRadixThreads) k_radix_scatter(int n, const uint64_t *__restrict__ kin,
+                                                                 const uint32_t *__restrict__ vin,
+                                                                 uint64_t *__restrict__ kout,
+                                                                 uint32_t *__restrict__ vout, int shift,
+                                                                 const unsigned *__restrict__ hist) {
+  __shared__ unsigned s_base[256];
+  __shared__ unsigned s_cnt[kRadixThreads / 32][256];
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  s_base[t] = hist[t * gridDim.x + blockIdx.x];
+#pragma unroll
+  for (int w = 0; w < kRadixThreads / 32; w++) s_cnt[w][t] = 0;
+  __syncthreads();
+  const int beg = blockIdx.x * kRadixChunk, end = min(n, beg + kRadixChunk);
+  const unsigned lt = (1u << lane) - 1u;
+  for (int base = beg; base < end; base += kRadixThreads) {
+    int i = base + t;
+    bool valid = i < end;
+    uint64_t k = valid ? kin[i] : 0;
+    uint32_t v = valid ? vin[i] : 0;
+    unsigned d = valid ? (unsigned)((k >> shift) & 255u) : 256u;
+    unsigned peers = __match_any_sync(0xffffffffu, d);
+    unsigned rank = __popc(peers & lt);
+    if (valid && rank == 0) s_cnt[warp][d] = __popc(peers);
+    __syncthreads();
+    {  // thread t owns digit t: exclusive prefix across warps
+      unsigned run = s_base[t];
+#pragma unroll
+      for (int w = 0; w < kRadixThreads / 32; w++) {
+        unsigned c = s_cnt[w][t];
+        s_cnt[w][t] = run;
+        run += c;
+      }
+      s_base[t] = run;
+    }
+    __syncthreads();
+    if (valid) {
+      unsigned o = s_cnt[warp][d] + rank;
+      kout[o] = k;
+      vout[o] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int w = 0; w < kRadixThreads / 32; w++) s_cnt[w][t] = 0;
+    __syncthreads();
+  }
+}
+
+size_t radix_scratch_bytes(int n) {
+  size_t nb = (size_t)(n + kRadixChunk - 1) / kRadixChunk;
+  if (nb == 0) nb = 1;
+  size_t b = 0;
+  b += ((size_t)n * 8 + 255) / 256 * 256;    // keys ping-pong
+  b += ((size_t)n * 4 + 255) / 256 * 256;    // vals ping-pong
+  b += (256 * nb * 4 + 255) / 256 * 256;     // histograms
+  return b;
+}
+
+// Stable sort of (keys, vals); result in keys/vals.  Returns launches.
+int radix_sort_u64(int n, uint64_t *keys, uint32_t *vals, void *scratch, cudaStream_t st) {
+  if (n <= 1) return 0;
+  int nb = (n + kRadixChunk - 1) / kRadixChunk;
+  char *p = (char *)scratch;
+  uint64_t *k2 = (uint64_t *)p;
+  p += ((size_t)n * 8 + 255) / 256 * 256;
+  uint32_t *v2 = (uint32_t *)p;
+  p += ((size_t)n * 4 + 255) / 256 * 256;
+  unsigned *hist = (unsigned *)p;
+  uint64_t *ka = keys, *kb = k2;
+  uint32_t *va = vals, *vb = v2;
+  int launches = 0;
+  for (int shift = 0; shift < 64; shift += 8) {
+    k_radix_hist<<<nb, kRadixThreads, 0, st>>>(n, ka, shift, hist);
+    k_radix_scan<<<1, 1024, 0, st>>>(256 * nb, hist);
+    k_radix_scatter<<<nb, kRadixThreads, 0, st>>>(n, ka, va, kb, vb, shift, hist);
+    launches += 3;
+    uint64_t *tk = ka; ka = kb; kb = tk;
+    uint32_t *tv = va; va = vb; vb = tv;
+  }
+  // 8 passes: the result is back in keys/vals
+  return launches;
+}
+
+// bounding box + Morton keys of positions (double4 records or separate x/y/z)
+int morton_keys(int n, const double4 *pos, const double *x, const double *y, const double *z, double *part,
+                double *box4, uint64_t *keys, uint32_t *vals, cudaStream_t st) {
+  int nb = 148 * 2;
+  if (nb * 256 > n) nb = (n + 255) / 256;
+  if (nb < 1) nb = 1;
+  k_bbox_partial<<<nb, 256, 0, st>>>(n, pos, x, y, z, part);
+  k_bbox_final<<<1, 32, 0, st>>>(nb, part, box4);
+  k_morton<<<(n + 255) / 256, 256, 0, st>>>(n, pos, x, y, z, box4, keys, vals);
+  return 3;
+}
+
+}  // namespace sph
+
+extern "C" size_t cudasph_sort_scratch_bytes(int n) { return sph::radix_scratch_bytes(n) + 148 * 2 * 6 * 8 + 256; }
+
+extern "C" int cudasph_radix_sort_u64(int n, uint64_t *keys, uint32_t *vals, void *scratch, void *stream) {
+  if (n < 0 || (n > 0 && (!keys || !vals || !scratch))) return SPH_ERR_ARG;
+  sph::radix_sort_u64(n, keys, vals, scratch, (cudaStream_t)stream);
+  SPH_CUDA_TRY(cudaGetLastError());
+  return SPH_OK;
+}
+
+extern "C" int cudasph_morton_keys(int n, const double *x, const double *y, const double *z, uint64_t *keys,
+                                   double *box4, void *stream) {
+  if (n <= 0) return n == 0 ? SPH_OK : SPH_ERR_ARG;
+  if (!x || !y || !z || !keys || !box4) return SPH_ERR_ARG;
+  double *part = nullptr;
+  SPH_CUDA_TRY(cudaMallocAsync((void **)&part, 148 * 2 * 6 * sizeof(double), (cudaStream_t)stream));
+  sph::morton_keys(n, nullptr, x, y, z, part, box4, keys, nullptr, (cudaStream_t)stream);
+  SPH_CUDA_TRY(cudaFreeAsync(part, (cudaStream_t)stream));
+  SPH_CUDA_TRY(cudaGetLastError());
+  return SPH_OK;
+}

@@ -1,0 +1,204 @@
+/*
+ * cudasph_b200.h -- C ABI of the B200 (sm_100a) SPH + self-gravity step.
+ *
+ * Two layers:
+ *
+ *  1. The native ("v2") API: an opaque context that owns a device-resident,
+ *     tree-ordered particle state (FP64 SoA of double4 records) and runs the
+ *     per-step pipeline of the reference driver (step.cpp:13-147):
+ *        sort -> predict -> [tree, solve_range, find_ngb, density, pressure,
+ *        hydro] -> gravity -> diagnostics -> timestep -> kick.
+ *     Every phase is also callable on its own.  All calls are ordered on the
+ *     context's CUDA stream; errors are returned as sph_status codes, and
+ *     device-side conditions (list overflow, walk-stack overflow, ...) are
+ *     accumulated in a status word read by cudasph_device_status().
+ *
+ *  2. The reference's own extern "C" symbols (CUDAsph.h:22-48, defined in
+ *     host_calls.cu:27-376), with the reference's signatures and float4
+ *     layouts, so that the reference's C++ driver links against this library
+ *     unchanged.  They are implemented on top of layer 1.
+ *
+ * All pointers are plain pointers; no C++ or torch types cross this boundary.
+ */
+#ifndef CUDASPH_B200_H_
+#define CUDASPH_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------------- */
+/* status codes (returned)                                                 */
+/* ---------------------------------------------------------------------- */
+typedef enum {
+  SPH_OK = 0,
+  SPH_ERR_CUDA = 1,      /* a CUDA runtime call failed (message: cudasph_last_error) */
+  SPH_ERR_ARG = 2,       /* invalid argument */
+  SPH_ERR_ALLOC = 3,     /* device allocation failed */
+  SPH_ERR_DEVICE = 4,    /* a device-side condition was raised (see the flags below) */
+  SPH_ERR_STATE = 5      /* a phase was called before its inputs exist */
+} sph_status;
+
+/* device-side condition flags (cudasph_device_status) */
+#define SPH_FLAG_NGB_OVERFLOW 0x1u      /* a neighbour list longer than ngb_cap was truncated */
+#define SPH_FLAG_STACK_OVERFLOW 0x2u    /* a tree walk ran out of stack (results incomplete) */
+#define SPH_FLAG_NONFINITE 0x4u         /* a non-finite EOS root or timestep was produced */
+#define SPH_FLAG_H_NOT_CONVERGED 0x8u   /* the h solve stopped at max_iter (reference behaviour) */
+
+/* ---------------------------------------------------------------------- */
+/* parameters                                                              */
+/* ---------------------------------------------------------------------- */
+typedef enum { SPH_EOS_IDEAL = 0, SPH_EOS_GAS_RADIATION = 1 } sph_eos_mode;
+typedef enum { SPH_SOFT_SPLINE = 0, SPH_SOFT_PLUMMER = 1 } sph_soft_mode;
+typedef enum { SPH_PREC_FP64 = 0, SPH_PREC_MIXED = 1 } sph_precision;
+
+typedef struct {
+  double n_target;   /* smoothed neighbour number; DESIRED_NGB, dev_solve_range.cu:14 */
+  double rel_err;    /* h-solve tolerance; CUDA_calls.cpp:4 */
+  int max_iter;      /* MAX_ITER, dev_solve_range.cu:15 */
+  double f_scale;    /* Newton step clamp in the bracket phase, dev_solve_range.cu:92 */
+  double av_alpha;   /* CUDA_calls.cpp:13 */
+  double av_beta;    /* CUDA_calls.cpp:14 */
+  double gamma;      /* adiabatic index (sound speed and ideal EOS), dev_art_visc.cu:15 */
+  int eos_mode;      /* sph_eos_mode; the reference has gas + radiation only */
+  int soft_mode;     /* sph_soft_mode; the reference softens with the spline at range */
+  double eps;        /* Plummer softening length */
+  int use_psi;       /* Psi (softening grad-h) term of dev_hydro_dots.cu:69-70; -1 = auto */
+  double cn1, cn2;   /* Courant factors, compute_timestep.cpp:4-5 */
+  double G;          /* gravitational constant (1 in the reference's solar units) */
+  int precision;     /* sph_precision */
+  int ngb_cap;       /* neighbour-list capacity per particle (0 = 4 * n_target + 32) */
+  int sort_every;    /* Morton re-sort period in steps (reference: 100, step.cpp:26) */
+} sph_params;
+
+/* particle fields, addressed in the caller's ORIGINAL particle order */
+typedef enum {
+  SPH_X = 0, SPH_Y, SPH_Z, SPH_RANGE,        /* bodies_pos {x,y,z,range = 2h} */
+  SPH_VX, SPH_VY, SPH_VZ, SPH_M,             /* bodies_vel {vx,vy,vz,mass} */
+  SPH_RHO, SPH_P, SPH_U, SPH_MU,             /* hydro_data {rho,P,u,mean_mu} */
+  SPH_DIVV, SPH_CURLV, SPH_OMEGA, SPH_PSI,   /* dots_data {divv,curlv,omega,psi} */
+  SPH_AX, SPH_AY, SPH_AZ, SPH_DU,            /* bodies_dots {ax,ay,az,du/dt} (total) */
+  SPH_GX, SPH_GY, SPH_GZ, SPH_PHI,           /* grav_data {gx,gy,gz,phi} */
+  SPH_VSIG,                                  /* hydro_data2.x (max signal speed) */
+  SPH_NFIELDS
+} sph_field;
+
+/* diagnostics vector of cudasph_statistics (system_statistics.cpp:4-84,
+ * step.cpp:99-117, compute_timestep.cpp:3-25) */
+enum {
+  SPH_ST_W = 0, SPH_ST_T, SPH_ST_U, SPH_ST_E,
+  SPH_ST_JX, SPH_ST_JY, SPH_ST_JZ,
+  SPH_ST_RCMX, SPH_ST_RCMY, SPH_ST_RCMZ,
+  SPH_ST_VCMX, SPH_ST_VCMY, SPH_ST_VCMZ,
+  SPH_ST_MTOT,
+  SPH_ST_FX, SPH_ST_FY, SPH_ST_FZ,           /* total force  sum m a */
+  SPH_ST_TX, SPH_ST_TY, SPH_ST_TZ,           /* total torque sum m x cross a */
+  SPH_ST_NGB_MEAN, SPH_ST_NGB_SIGMA, SPH_ST_NGB_MIN, SPH_ST_NGB_MAX,
+  SPH_ST_DT_VEL, SPH_ST_DT_ETH, SPH_ST_DT,   /* compute_timestep minima */
+  SPH_ST_TIME, SPH_ST_DT_OLD,
+  SPH_NSTATS
+};
+
+typedef struct sph_ctx sph_ctx;
+
+/* defaults = the reference's constants (N 24, rel_err 1e-3, MAX_ITER 20,
+ * f_scale 0.1, alpha 1, beta 2, gamma 5/3, gas+radiation EOS, spline
+ * softening, Courant 0.3/0.2, G 1), FP64, sort every step. */
+sph_params cudasph_default_params(void);
+
+/* lifecycle */
+int cudasph_create(const sph_params *params, int n, int device, sph_ctx **out);
+int cudasph_destroy(sph_ctx *ctx);
+const char *cudasph_last_error(void);
+int cudasph_set_params(sph_ctx *ctx, const sph_params *params);
+int cudasph_get_params(const sph_ctx *ctx, sph_params *out);
+int cudasph_num_particles(const sph_ctx *ctx);
+
+/* state exchange; `on_device` = 1 when src/dst is a device pointer.
+ * Arrays are n doubles in the caller's original order. */
+int cudasph_set_field(sph_ctx *ctx, int field, const double *src, int on_device);
+int cudasph_get_field(sph_ctx *ctx, int field, double *dst, int on_device);
+/* whole-state exchange in one call: fields[k] for k < SPH_NFIELDS (NULL = skip) */
+int cudasph_set_state(sph_ctx *ctx, const double *const *fields, int on_device);
+int cudasph_get_state(sph_ctx *ctx, double *const *fields, int on_device);
+int cudasph_get_n_ngb(sph_ctx *ctx, int *dst, int on_device);
+/* the tree (sorted) slot of each original particle: slot_of[orig] */
+int cudasph_get_order(sph_ctx *ctx, int *sorted_ids_host);
+int cudasph_set_time(sph_ctx *ctx, double time, double dt);
+int cudasph_get_time(sph_ctx *ctx, double *time, double *dt);
+
+/* neighbour lists in original ids: counts[n]; offsets[n+1] (int64) and
+ * list[offsets[n]] ascending by tree slot.  Pass list = NULL to get the
+ * counts and offsets only. */
+int cudasph_get_neighbours(sph_ctx *ctx, int *counts, int64_t *offsets, int *list);
+
+/* pipeline phases (stream ordered; see step.cpp:13-147 for the order) */
+int cudasph_sort(sph_ctx *ctx);              /* Morton keys + radix sort + permute (sort_bodies.cpp:119) */
+int cudasph_predict(sph_ctx *ctx);           /* step.cpp:38-61 */
+int cudasph_build_tree(sph_ctx *ctx);        /* kd_tree.cpp:97-128 replacement */
+int cudasph_solve_range(sph_ctx *ctx);       /* dev_solve_range.cu:174 */
+int cudasph_find_ngb(sph_ctx *ctx);          /* dev_find_ngb.cu:75 */
+int cudasph_density(sph_ctx *ctx);           /* dev_density_loop.cu:88 */
+int cudasph_pressure(sph_ctx *ctx);          /* dev_compute_pressure.cu:99 */
+int cudasph_hydro(sph_ctx *ctx);             /* dev_hydro_dots.cu:86 + sph_accelerations.cpp:106-114 */
+int cudasph_sph_accelerations(sph_ctx *ctx); /* tree .. hydro, sph_accelerations.cpp:3-121 */
+int cudasph_gravity(sph_ctx *ctx);           /* sph_grav_kernel.cu:179 */
+int cudasph_finish(sph_ctx *ctx);            /* a += g, diagnostics, timestep (step.cpp:96-127) */
+int cudasph_kick(sph_ctx *ctx);              /* step.cpp:128-134 */
+int cudasph_step(sph_ctx *ctx);              /* the whole step */
+int cudasph_steps(sph_ctx *ctx, int k);      /* k whole steps */
+
+/* End-to-end step through host buffers, the way the reference driver owns
+ * its state: copy the fields in (host, pinned or not), run one step, copy
+ * the fields out.  fields_in/fields_out as in cudasph_set_state. */
+int cudasph_step_host(sph_ctx *ctx, const double *const *fields_in, double *const *fields_out);
+
+int cudasph_synchronize(sph_ctx *ctx);
+int cudasph_statistics(sph_ctx *ctx, double *stats /* SPH_NSTATS */);
+/* read and clear the device condition flags (synchronizes) */
+int cudasph_device_status(sph_ctx *ctx, unsigned *flags);
+/* number of h-solve evaluations per particle of the last solve (original order) */
+int cudasph_get_solve_evals(sph_ctx *ctx, int *dst);
+
+/* instrumentation: CUDA-event time of each phase, summed since the last reset */
+enum {
+  SPH_PH_SORT = 0, SPH_PH_PREDICT, SPH_PH_TREE, SPH_PH_SOLVE, SPH_PH_FIND, SPH_PH_DENSITY,
+  SPH_PH_PRESSURE, SPH_PH_HYDRO, SPH_PH_GRAVITY, SPH_PH_FINISH, SPH_PH_KICK, SPH_NPHASES
+};
+int cudasph_set_profiling(sph_ctx *ctx, int on);
+int cudasph_phase_times(sph_ctx *ctx, double *ms /* SPH_NPHASES */, int *launches /* SPH_NPHASES */);
+int cudasph_reset_counters(sph_ctx *ctx);
+/* kernels launched by this context since the last reset */
+long long cudasph_kernel_launches(const sph_ctx *ctx);
+
+/* ---------------------------------------------------------------------- */
+/* stand-alone operators on caller-owned device buffers                    */
+/* ---------------------------------------------------------------------- */
+/* Morton keys (21 bits per dimension in the bounding cube) and a stable
+ * LSD radix sort of (key, value) pairs; `scratch` must hold
+ * cudasph_sort_scratch_bytes(n) bytes.  Results land in keys/vals. */
+size_t cudasph_sort_scratch_bytes(int n);
+int cudasph_morton_keys(int n, const double *x, const double *y, const double *z, uint64_t *keys,
+                        double *box4 /* device, 4 doubles: lo xyz, scale */, void *stream);
+int cudasph_radix_sort_u64(int n, uint64_t *keys, uint32_t *vals, void *scratch, void *stream);
+
+/* direct-N gravity of n sources on themselves: pos4 = {x,y,z,m}, range =
+ * smoothing ranges (spline mode), out4 = {gx,gy,gz,phi}; double buffers. */
+int cudasph_gravity_direct(int n, const double *pos4, const double *range, double *out4, int soft_mode,
+                           double eps, double G, int precision, void *stream);
+
+/* ---------------------------------------------------------------------- */
+/* the reference's extern "C" boundary (CUDAsph.h:22-48)                   */
+/* ---------------------------------------------------------------------- */
+#ifndef CUDASPH_B200_NO_LEGACY
+#include "cudasph_b200_legacy.h"
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUDASPH_B200_H_ */

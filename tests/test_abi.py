@@ -1,0 +1,96 @@
+"""The C ABI library: loads, exports every symbol the headers declare, carries
+the reference's constants as defaults, and validates arguments on the host.
+These tests make no compute call and run without a GPU."""
+import ctypes as C
+import os
+import subprocess
+
+import pytest
+
+from cudasph_b200 import _capi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADERS = [os.path.join(ROOT, "include", h) for h in ("cudasph_b200.h", "cudasph_b200_legacy.h")]
+
+# the reference's extern "C" symbols (CUDAsph.h:22-48, radixsort.cuh:59-61)
+REFERENCE_SYMBOLS = [
+    "initCUDA", "allocateCUDAarray", "deleteCUDAarray", "copyArrayToDevice", "copyArrayFromDevice",
+    "compute_CUDA_gravity", "allocateNBodyArrays", "deleteNBodyArrays", "zallocateNBodyArrays",
+    "zdeleteNBodyArrays", "zcopyArrayFromDevice", "zcopyArrayToDevice", "host_solve_range",
+    "host_sph_accelerations", "get_device_count", "cuda_set_device", "cuda_set_device0", "cuda_get_device",
+    "RadixSort",
+]
+
+
+def _exports():
+    out = subprocess.run(["nm", "-D", "--defined-only", _capi.LIB_PATH], capture_output=True, text=True, check=True)
+    return {line.split()[-1] for line in out.stdout.splitlines() if line.strip()}
+
+
+def test_library_loads():
+    _capi.lib()
+
+
+def test_every_declared_symbol_is_exported():
+    declared = _capi.declared_symbols(HEADERS)
+    assert len(declared) > 40
+    ex = _exports()
+    missing = [s for s in declared if s not in ex]
+    assert not missing, missing
+
+
+def test_reference_boundary_is_exported():
+    ex = _exports()
+    assert all(s in ex for s in REFERENCE_SYMBOLS)
+    assert set(REFERENCE_SYMBOLS) <= set(_capi.declared_symbols(HEADERS))
+
+
+def test_default_params_are_the_reference_constants():
+    p = _capi.lib().cudasph_default_params()
+    assert p.n_target == 24.0        # DESIRED_NGB, dev_solve_range.cu:14
+    assert p.rel_err == 1e-3         # CUDA_calls.cpp:4
+    assert p.max_iter == 20          # MAX_ITER, dev_solve_range.cu:15
+    assert p.f_scale == 0.1          # dev_solve_range.cu:92
+    assert (p.av_alpha, p.av_beta) == (1.0, 2.0)  # CUDA_calls.cpp:13-14
+    assert abs(p.gamma - 5.0 / 3.0) < 1e-15
+    assert (p.cn1, p.cn2) == (0.3, 0.2)  # compute_timestep.cpp:4-5
+    assert p.eos_mode == 1 and p.soft_mode == 0 and p.precision == 0
+
+
+@pytest.mark.parametrize("field,value", [("n_target", 0.0), ("rel_err", -1.0), ("eos_mode", 7), ("soft_mode", 3),
+                                         ("precision", 5), ("gamma", 1.0), ("ngb_cap", -1)])
+def test_invalid_params_rejected_before_any_device_call(field, value):
+    L = _capi.lib()
+    p = L.cudasph_default_params()
+    setattr(p, field, value)
+    h = C.c_void_p()
+    assert L.cudasph_create(C.byref(p), 100, 0, C.byref(h)) == 2  # SPH_ERR_ARG
+    assert not h.value
+
+
+def test_plummer_needs_positive_eps():
+    L = _capi.lib()
+    p = L.cudasph_default_params()
+    p.soft_mode = 1
+    p.eps = 0.0
+    h = C.c_void_p()
+    assert L.cudasph_create(C.byref(p), 10, 0, C.byref(h)) == 2
+
+
+def test_null_context_calls_return_arg_error():
+    L = _capi.lib()
+    for name in ("sort", "predict", "build_tree", "solve_range", "find_ngb", "density", "hydro", "gravity",
+                 "finish", "kick", "step"):
+        assert getattr(L, "cudasph_" + name)(None) == 2, name
+    assert L.cudasph_destroy(None) == 0
+
+
+def test_create_without_gpu_reports_cuda_error():
+    from conftest import gpu_available
+    if gpu_available():
+        pytest.skip("a GPU is present")
+    L = _capi.lib()
+    p = L.cudasph_default_params()
+    h = C.c_void_p()
+    assert L.cudasph_create(C.byref(p), 100, 0, C.byref(h)) == 1  # SPH_ERR_CUDA
+    assert b"failed" in L.cudasph_last_error()
