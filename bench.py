@@ -1,0 +1,388 @@
+#!/usr/bin/env python
+"""Benchmark of the SPH + self-gravity step (one JSON line on stdout).
+
+Workload (the configuration the headline metric is quoted on): N = 1,048,576
+particles, two n = 1.5 polytropes of 524,288 particles each (M = R = G = 1),
+centres 4R apart, approaching head on at relative speed 1.0; ideal gas +
+radiation EOS with mu = 0.62; N_ngb = 64; Plummer softening eps = 0.002;
+mixed precision (FP32 pair terms on FP64 anchors, compensated sums, FP64 h
+solve / EOS root / integration / reductions).  Seeded synthetic data: the
+reference has no dataset.
+
+A step is one whole time step of the pipeline (sort, predict, tree,
+solve_range, find_ngb, density, pressure, hydro, gravity, diagnostics,
+timestep, kick) with the state resident in HBM.  The state (~500 MB) is far
+larger than L2, so no flush is needed between steps.
+
+  value        particle-steps/s of the mixed step (device time, CUDA events,
+               max over ranks)
+  e2e          the same through the C ABI with host buffers: every step copies
+               the state in from pinned host memory and the result out
+  fp64         the plain FP64 step on the same workload, and the mixed/fp64
+               ratio; errors = mixed vs FP64 accelerations at the same state
+  roofline     the direct-N gravity kernel on the FP32 FMA pipe: 20 flops per
+               pair interaction x N^2 per launch / launch time, against the
+               FP32 FMA peak measured in the same run
+  cpu_baseline the reference's own code built for the host CPU (oracle/_ref),
+               on a bounded sample (see 'sample')
+
+--impl reference times only the reference's CPU build on the same workload.
+Under torchrun (N > 1) every rank runs an independent replica (the path is
+data-parallel over independent simulations here); rank 0 prints.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s at N=1M, mixed vs FP64 at stated error; adjoint/forward cost"
+UNIT = "particle-steps/s"
+
+
+def workload_ic(n_total: int, seed: int = 12345 + 3):
+    from cudasph_b200 import ics
+    return ics.two_star_collision(n_total // 2, separation=4.0, rel_speed=1.0, n_poly=1.5, n_ngb=64.0, seed=seed,
+                                  mu=0.62)
+
+
+WORKLOAD_PARAMS = dict(n_target=64.0, eos_mode=1, soft_mode=1, eps=0.002)
+
+
+def workload_name(n):
+    return (f"two n=1.5 polytropes head-on (2 x {n // 2}), N={n}, gas+radiation EOS mu=0.62, N_ngb=64, "
+            f"Plummer eps=0.002")
+
+
+# ----------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi samples during the timed region (every 200 ms)."""
+
+    Q = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.proc = None
+        self.f = None
+
+    def __enter__(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or self.f is None:
+            return None
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for line in fh:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 8:
+                    continue
+                if self.uuid and parts[0] != self.uuid:
+                    continue
+                try:
+                    rows.append((float(parts[1]), float(parts[2]), parts[4:8]))
+                except ValueError:
+                    continue
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for _, _, r in rows for k in range(4) if r[k].lower() == "active"})
+        sm = [r[0] for r in rows]
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(rows[0][1]), "reasons": reasons,
+                "samples": len(rows)}
+
+
+def gpu_uuid():
+    try:
+        import torch
+        u = str(torch.cuda.get_device_properties(torch.cuda.current_device()).uuid)
+        return u if u.startswith("GPU-") else "GPU-" + u
+    except Exception:
+        return None
+
+
+# ----------------------------------------------------------------------------
+def time_steps(sim, steps, warmup):
+    """Device time of `steps` whole steps (CUDA events on the context stream)."""
+    sim.step(warmup)
+    sim.synchronize()
+    sim.reset_counters()
+    sim.set_profiling(True)
+    t0 = time.perf_counter()
+    sim.step(steps)
+    sim.synchronize()
+    wall = time.perf_counter() - t0
+    ph = sim.phase_times()
+    sim.set_profiling(False)
+    dev_ms = sum(v[0] for v in ph.values())
+    return dev_ms, wall, ph, sim.kernel_launches()
+
+
+def rms_rel(a, b):
+    return float(np.sqrt(np.mean(np.sum((a - b) ** 2, axis=1)) / np.mean(np.sum(b ** 2, axis=1))))
+
+
+def traffic_from_profiles(kernel_tag: str, n: int):
+    """Per-launch DRAM bytes of a kernel from the committed ncu summary
+    (profiles/<kernel_tag>.md, line 'traffic_bytes_per_launch_at_N=<n0>: <B>'),
+    scaled to n by the units processed (N^2 pair interactions stream the
+    sources from L2, DRAM traffic grows ~ N * tiles)."""
+    path = os.path.join(ROOT, "profiles", kernel_tag + ".md")
+    if not os.path.exists(path):
+        return None
+    import re
+    txt = open(path).read()
+    m = re.search(r"traffic_bytes_per_launch_at_N=(\d+):\s*([0-9.eE+]+)", txt)
+    if not m:
+        return None
+    n0, b0 = int(m.group(1)), float(m.group(2))
+    return b0 * (n / n0) ** 2 if n != n0 else b0
+
+
+def cpu_reference_sample(ic, n_grav_targets=256):
+    from oracle import oracle as O
+    if not O.ref_available():
+        return None
+    R = O.RefPipeline(ic)
+    t = R.time_step(n_grav_targets=n_grav_targets)
+    return t, O.ref().ref_num_threads()
+
+
+def run_ours(args, rank, world):
+    import torch
+    from cudasph_b200.simulation import Simulation, make_params
+    from cudasph_b200 import _capi
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    n = args.n
+    ic = workload_ic(n)
+    kw = dict(WORKLOAD_PARAMS)
+    if args.fp64_only:
+        kw["precision"] = 0
+    else:
+        kw["precision"] = 1
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    # FMA-pipe peaks measured in this run (roofline denominators)
+    L = _capi.lib()
+    peak32 = L.cudasph_fma_peak(1, 4096, None)
+    peak64 = L.cudasph_fma_peak(0, 1024, None)
+
+    # --- the mixed (headline) step -------------------------------------------------
+    sim = Simulation(ic, make_params(**kw), device=dev)
+    sim.step(args.warmup)
+    sim.synchronize()
+    barrier()
+    with ClockSampler(gpu_uuid()) as clk:
+        dev_ms, wall, ph, launches = time_steps(sim, args.steps, 0)
+        barrier()
+    clocks = clk.summary()
+    flags = sim.device_status()
+    ms_step = dev_ms / args.steps
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms_step], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_step = float(t.item())
+    value = world * n * 1000.0 / ms_step
+    stats = sim.system_statistics()
+    gms, gl = ph["gravity"]
+    grav_ms = gms / max(gl, 1)
+    sim.close()
+
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64" if args.fp64_only else "f32+f64", "data": "synthetic (seeded)",
+           "config": {"workload": workload_name(n), "n_particles": n, "precision": "fp64" if args.fp64_only else
+                      "mixed", "l2": "state (~%.0f MB) larger than L2; no flush" % (n * 500 / 1e6),
+                      "parallelism": "replicas" if world > 1 else "single GPU"},
+           "gpu_launches": int(launches),
+           "phase_ms_per_step": {k: round(v[0] / args.steps, 4) for k, v in ph.items()},
+           "device_flags": flags}
+    if clocks:
+        out["clocks"] = clocks
+    if rank != 0:
+        return None
+
+    flops = 20.0 * n * n
+    prec_peak = peak64 if args.fp64_only else peak32
+    achieved = flops / (grav_ms * 1e-3)
+    tag = "gravity_fp64_plummer" if args.fp64_only else "gravity_mixed_plummer"
+    out["roofline"] = {"kernel": tag, "bound": "fp64_pipe" if args.fp64_only else "fp32_pipe",
+                       "achieved": achieved / 1e12, "peak": prec_peak / 1e12, "unit": "TFLOP/s",
+                       "frac": achieved / prec_peak, "traffic": traffic_from_profiles(tag, n),
+                       "peak_source": "FMA-chain probe measured in this run (the pool's measured-peaks file "
+                                      "has HBM and bf16 tensor figures only)",
+                       "flops_per_launch": flops, "launch_ms": grav_ms,
+                       "interactions_per_s": n * n / (grav_ms * 1e-3)}
+    out["stats_last_step"] = {k: stats[k] for k in ("E", "W", "T", "U", "dt", "ngb_mean", "ngb_min", "ngb_max")}
+
+    # --- FP64 comparison and errors ----------------------------------------------
+    if not args.fp64_only and args.fp64_steps > 0:
+        kw64 = dict(kw, precision=0)
+        s64 = Simulation(ic, make_params(**kw64), device=dev)
+        s32 = Simulation(ic, make_params(**kw), device=dev)
+        s64.step(1)
+        s32.step(1)
+        a64 = np.stack([s64.get(k) for k in ("ax", "ay", "az")], 1)
+        a32 = np.stack([s32.get(k) for k in ("ax", "ay", "az")], 1)
+        g64 = np.stack([s64.get(k) for k in ("gx", "gy", "gz")], 1)
+        g32 = np.stack([s32.get(k) for k in ("gx", "gy", "gz")], 1)
+        p64, p32 = s64.get("phi"), s32.get("phi")
+        r64, r32 = s64.get("rho"), s32.get("rho")
+        du64, du32 = s64.get("du"), s32.get("du")
+        errors = {"rms_force_rel": rms_rel(a32, a64), "rms_gravity_rel": rms_rel(g32, g64),
+                  "max_phi_rel": float(np.max(np.abs(p32 / p64 - 1))),
+                  "max_rho_rel": float(np.max(np.abs(r32 / r64 - 1))),
+                  "rms_du_rel": float(np.sqrt(np.mean((du32 - du64) ** 2) / max(np.mean(du64 ** 2), 1e-300))),
+                  "rms_hydro_rel": rms_rel(a32 - g32, a64 - g64),
+                  "rms_force_rel_to_gravity_scale": float(np.sqrt(np.mean(np.sum((a32 - a64) ** 2, 1))
+                                                                  / np.mean(np.sum(g64 ** 2, 1)))),
+                  "against": "FP64 GPU step (equal to the FP64 oracle to 1e-12 in the parity tests) at the "
+                             "same state, first step"}
+        s32.close()
+        dms64, _, ph64, _ = time_steps(s64, args.fp64_steps, 1)
+        ms64 = dms64 / args.fp64_steps
+        g64ms = ph64["gravity"][0] / max(ph64["gravity"][1], 1)
+        s64.close()
+        out["fp64"] = {"value": n * 1000.0 / ms64, "ms_per_step": ms64, "steps": args.fp64_steps,
+                       "gravity_ms": g64ms, "gravity_frac_of_fp64_peak": flops / (g64ms * 1e-3) / peak64}
+        out["mixed_over_fp64"] = ms64 / ms_step
+        out["errors"] = errors
+
+    # --- end to end through the C ABI with host buffers ----------------------------
+    if args.e2e_steps > 0:
+        from cudasph_b200._capi import FIELDS
+        ins = ("x", "y", "z", "range", "vx", "vy", "vz", "m", "u", "mu", "ax", "ay", "az", "du")
+        outs = ins + ("rho", "P")
+        sim = Simulation(ic, make_params(**kw), device=dev)
+        sim.step(2)
+        sim.synchronize()
+        host_in = {k: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy() for k in ins}
+        host_out = {k: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy() for k in outs}
+        for k in ins:
+            host_in[k][:] = sim.get(k)
+        sim.step_host(host_in, host_out)  # warm
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            for k in ins:
+                host_in[k][:] = host_out[k]
+            sim.step_host(host_in, host_out)
+        e2e_s = time.perf_counter() - t0
+        sim.close()
+        out["e2e"] = {"value": n * args.e2e_steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 8 * n * len(ins),
+                      "d2h_bytes_per_step": 8 * n * len(outs), "steps": args.e2e_steps,
+                      "api": "cudasph_step_host (C ABI), pinned host buffers, wall clock"}
+
+    # --- CPU baseline: the reference's own code on the host ----------------------------
+    if args.cpu_baseline:
+        r = cpu_reference_sample(ic, n_grav_targets=args.cpu_grav_targets)
+        if r is not None:
+            t, cores = r
+            out["cpu_baseline"] = {
+                "value": n / t["step"], "unit": UNIT, "cores": cores, "kind": "reference",
+                "sample": (f"reference device code + kd-tree built for the CPU (oracle/_ref), one step on the "
+                           f"same {n}-particle state: kd-tree build, solve_range, find_ngb, density, pressure, "
+                           f"hydro + scatter over all particles, gravity for {args.cpu_grav_targets} sampled "
+                           f"targets x {n} sources extrapolated to {n}; the reference's compiled-in "
+                           f"DESIRED_NGB=24 and spline softening"),
+                "phase_s": {k: round(v, 3) for k, v in t.items()}}
+    return out
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    from oracle import oracle as O
+    if not O.ref_available():
+        return {"impl": "reference", "unavailable": "oracle/_ref (the reference built for the host CPU) is missing"}
+    n = args.n
+    ic = workload_ic(n)
+    times = []
+    for i in range(args.warmup + args.steps):
+        R = O.RefPipeline(ic)
+        t = R.time_step(n_grav_targets=args.cpu_grav_targets, seed=i)
+        if i >= args.warmup:
+            times.append(t["step"])
+    ms = 1000.0 * float(np.mean(times))
+    value = n * 1000.0 / ms
+    cores = O.ref().ref_num_threads()
+    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)", "impl": "reference",
+            "config": {"workload": workload_name(n), "n_particles": n, "precision": "reference FP32 + float-float"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                             "sample": f"per step: full SPH pass over {n} particles with the reference's code "
+                                       f"(DESIRED_NGB=24, spline softening), gravity on {args.cpu_grav_targets} "
+                                       f"sampled targets x {n} sources extrapolated"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=1 << 20)
+    ap.add_argument("--fp64-only", action="store_true")
+    ap.add_argument("--fp64-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-grav-targets", type=int, default=256)
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    args = ap.parse_args()
+    assert args.warmup >= 3 or args.impl == "reference" or os.environ.get("BENCH_ALLOW_SHORT_WARMUP")
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1 and args.impl == "ours":
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    try:
+        out = run_ours(args, rank, world) if args.impl == "ours" else run_reference(args, rank, world)
+    finally:
+        if world > 1 and args.impl == "ours":
+            import torch.distributed as dist
+            dist.destroy_process_group()
+    if out is not None and rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

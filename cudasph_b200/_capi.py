@@ -86,6 +86,8 @@ def lib():
     L.cudasph_morton_keys.argtypes = [ip, vp, vp, vp, vp, vp, vp]
     L.cudasph_radix_sort_u64.argtypes = [ip, vp, vp, vp, vp]
     L.cudasph_gravity_direct.argtypes = [ip, vp, vp, vp, ip, dp, dp, ip, vp]
+    L.cudasph_fma_peak.argtypes = [ip, ip, vp]
+    L.cudasph_fma_peak.restype = C.c_double
     _lib = L
     return L
 

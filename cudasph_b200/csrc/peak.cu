@@ -1,0 +1,59 @@
+// peak.cu -- FMA-pipe throughput probe, the denominator of the gravity
+// roofline.  The measured-peaks file of the pool carries HBM and tensor-core
+// figures only, while the direct-N gravity inner loop runs on the FP32 (mixed
+// form) or FP64 (plain form) FMA pipe, so its peak is measured in the same
+// run: every thread advances 8 independent FMA chains; the grid fills every
+// SM several times over.
+#include "common.cuh"
+
+namespace sph {
+
+template <class R>
+__global__ void __launch_bounds__(256) k_fma_peak(int iters, R a, R b, R *out) {
+  R x0 = (R)threadIdx.x, x1 = x0 + (R)1, x2 = x0 + (R)2, x3 = x0 + (R)3;
+  R x4 = x0 + (R)4, x5 = x0 + (R)5, x6 = x0 + (R)6, x7 = x0 + (R)7;
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+      x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
+      x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
+    }
+  }
+  const R s = ((x0 + x1) + (x2 + x3)) + ((x4 + x5) + (x6 + x7));
+  if (s == (R)-1.2345) out[blockIdx.x] = s;  // keeps the chains alive
+}
+
+}  // namespace sph
+
+// Runs the probe on `stream` and returns the achieved FLOP/s (2 per FMA)
+// measured with CUDA events; precision 1 = FP32, 0 = FP64.
+extern "C" double cudasph_fma_peak(int precision, int iters, void *stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int blocks = sms * 8, threads = 256;
+  void *out = nullptr;
+  if (cudaMallocAsync(&out, sizeof(double) * blocks, st) != cudaSuccess) return -1;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  // warm up, then time
+  for (int rep = 0; rep < 2; rep++) {
+    cudaEventRecord(e0, st);
+    if (precision == 1)
+      sph::k_fma_peak<float><<<blocks, threads, 0, st>>>(iters, 0.999999f, 1e-7f, (float *)out);
+    else
+      sph::k_fma_peak<double><<<blocks, threads, 0, st>>>(iters, 0.999999999, 1e-12, (double *)out);
+    cudaEventRecord(e1, st);
+  }
+  cudaEventSynchronize(e1);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFreeAsync(out, st);
+  cudaStreamSynchronize(st);
+  const double flops = 2.0 * 8 * 16 * (double)iters * blocks * threads;
+  return ms > 0 ? flops / (ms * 1e-3) : -1;
+}

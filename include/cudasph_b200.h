@@ -190,6 +190,10 @@ int cudasph_radix_sort_u64(int n, uint64_t *keys, uint32_t *vals, void *scratch,
 int cudasph_gravity_direct(int n, const double *pos4, const double *range, double *out4, int soft_mode,
                            double eps, double G, int precision, void *stream);
 
+/* FMA-pipe throughput probe (FLOP/s, 2 per FMA) on `stream`: precision 1 =
+ * FP32, 0 = FP64.  The roofline denominator of the direct-N gravity loop. */
+double cudasph_fma_peak(int precision, int iters, void *stream);
+
 /* ---------------------------------------------------------------------- */
 /* the reference's extern "C" boundary (CUDAsph.h:22-48)                   */
 /* ---------------------------------------------------------------------- */

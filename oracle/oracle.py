@@ -332,6 +332,34 @@ class RefPipeline:
         ref().ref_add_ngb_acc(n, self.pos, self.n_ngb, self.off, self.lst, self.ngb_acc, self.dots)
         return self.dots.copy(), self.vsig.copy()
 
+    def time_step(self, n_grav_targets: int = 256, seed: int = 0) -> dict:
+        """Wall-clock of one reference step on this state (sph_accelerations.cpp:
+        3-121 + CUDA_gravity.cpp:3-71): kd-tree build (the reference's host
+        code, single thread), solve_range / find_ngb / density / pressure /
+        hydro / j-side scatter over all particles (OpenMP over particles), and
+        gravity for a seeded sample of n_grav_targets bodies against all n,
+        extrapolated to n.  Returns the per-phase seconds and 'step'."""
+        import time
+        t = {}
+        t0 = time.perf_counter(); self.kdtree(); t["tree"] = time.perf_counter() - t0
+        t0 = time.perf_counter(); self.solve_range(); t["solve_range"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        n = self.n
+        self.off = np.zeros(n + 1, np.int32)
+        tot = ref().ref_ngb_offsets(n, self.n_ngb + 4, self.off)
+        self.lst = np.full(tot, -1, np.int32)
+        ref().ref_find_ngb(n, self.pos, self.nodes, self.off, self.lst, None)
+        t["find_ngb"] = time.perf_counter() - t0
+        t0 = time.perf_counter(); self.density(); t["density"] = time.perf_counter() - t0
+        t0 = time.perf_counter(); self.pressure(); t["pressure"] = time.perf_counter() - t0
+        t0 = time.perf_counter(); self.hydro_dots(); t["hydro"] = time.perf_counter() - t0
+        tg = np.random.default_rng(seed).choice(n, size=min(n_grav_targets, n), replace=False).astype(np.int32)
+        t0 = time.perf_counter(); self.gravity(tg); tgs = time.perf_counter() - t0
+        t["gravity_sample"] = tgs
+        t["gravity"] = tgs * n / tg.size
+        t["step"] = sum(v for k, v in t.items() if k != "gravity_sample")
+        return t
+
     def gravity(self, targets=None):
         n = self.n
         gpos = _f4(self.pos[:, 0], self.pos[:, 1], self.pos[:, 2], self.vel[:, 3])
