@@ -153,8 +153,9 @@ def rms_rel(a, b):
 def traffic_from_profiles(kernel_tag: str, n: int):
     """Per-launch DRAM bytes of a kernel from the committed ncu summary
     (profiles/<kernel_tag>.md, line 'traffic_bytes_per_launch_at_N=<n0>: <B>'),
-    scaled to n by the units processed (N^2 pair interactions stream the
-    sources from L2, DRAM traffic grows ~ N * tiles)."""
+    scaled to n in proportion to the particles: the 32-byte source records
+    (32 MB at N = 1M) stay resident in L2 across the N^2 interactions, so DRAM
+    sees each record once per launch."""
     path = os.path.join(ROOT, "profiles", kernel_tag + ".md")
     if not os.path.exists(path):
         return None
@@ -164,7 +165,7 @@ def traffic_from_profiles(kernel_tag: str, n: int):
     if not m:
         return None
     n0, b0 = int(m.group(1)), float(m.group(2))
-    return b0 * (n / n0) ** 2 if n != n0 else b0
+    return b0 * (n / n0)
 
 
 def cpu_reference_sample(ic, n_grav_targets=256):

@@ -152,7 +152,7 @@ int check_params(const sph_params *p) {
   if (p->soft_mode != SPH_SOFT_SPLINE && p->soft_mode != SPH_SOFT_PLUMMER) return SPH_ERR_ARG;
   if (p->soft_mode == SPH_SOFT_PLUMMER && !(p->eps > 0)) return SPH_ERR_ARG;
   if (p->precision != SPH_PREC_FP64 && p->precision != SPH_PREC_MIXED) return SPH_ERR_ARG;
-  if (p->ngb_cap < 0 || p->sort_every < 0) return SPH_ERR_ARG;
+  if (p->ngb_cap < 0 || p->sort_every < 0 || p->mixed_sph < 0 || p->mixed_sph > 3) return SPH_ERR_ARG;
   if (!(p->gamma > 1)) return SPH_ERR_ARG;
   return SPH_OK;
 }
@@ -215,6 +215,7 @@ extern "C" sph_params cudasph_default_params(void) {
   p.precision = SPH_PREC_FP64;
   p.ngb_cap = 0;
   p.sort_every = 1;
+  p.mixed_sph = 3;
   return p;
 }
 
@@ -556,7 +557,7 @@ extern "C" int cudasph_density(sph_ctx *c) {
   SPH_CUDA_TRY(cudaSetDevice(c->device));
   PhaseScope ps(c, SPH_PH_DENSITY);
   HydroArgs a = hydro_args(c);
-  if (c->p.precision == SPH_PREC_MIXED) LAUNCHED(launch_density_mixed(a, c->st));
+  if (c->p.precision == SPH_PREC_MIXED && (c->p.mixed_sph & 1)) LAUNCHED(launch_density_mixed(a, c->st));
   else LAUNCHED(launch_density(a, c->st));
   c->density_ok = true;
   SPH_CUDA_TRY(cudaGetLastError());
@@ -580,7 +581,7 @@ extern "C" int cudasph_hydro(sph_ctx *c) {
   Fields &F = c->f[c->cur];
   SPH_CUDA_TRY(cudaMemsetAsync(F.dots, 0, sizeof(double4) * c->n, c->st));
   HydroArgs a = hydro_args(c);
-  if (c->p.precision == SPH_PREC_MIXED) LAUNCHED(launch_hydro_mixed(a, c->st));
+  if (c->p.precision == SPH_PREC_MIXED && (c->p.mixed_sph & 2)) LAUNCHED(launch_hydro_mixed(a, c->st));
   else LAUNCHED(launch_hydro(a, c->st));
   SPH_CUDA_TRY(cudaGetLastError());
   return SPH_OK;

@@ -292,6 +292,127 @@ __global__ void __launch_bounds__(kGThreads) k_grav_f32(int n, const double4 *__
   }
 }
 
+// --------------------- mixed (FP32), packed f32x2 form ----------------------
+// Plummer-softened mixed kernel on Blackwell's packed FP32 instructions
+// (add/mul/fma.rn.f32x2): each instruction advances two i-particles against
+// the same source, which halves the FP32 instruction count per interaction
+// (13 packed + 2 MUFU per two interactions) and moves the loop from the
+// warp-issue limit to the FMA-pipe limit.  Sources are stored in shared
+// memory pre-duplicated ({x,x}, {y,y}, {z,z}, {m,m}) so a source costs two
+// 16-byte shared loads per thread and no repacking.  Padding sources beyond n
+// have m = 0 at the anchor; eps > 0 keeps their r^2 > 0, so every tile is a
+// full tile.
+typedef unsigned long long f32x2;
+
+__device__ __forceinline__ f32x2 pk2(float a, float b) {
+  f32x2 r;
+  asm("mov.b64 %0, {%1,%2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ void upk2(f32x2 v, float &a, float &b) {
+  asm("mov.b64 {%0,%1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ f32x2 sub2(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
+  f32x2 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+
+template <int RP>  // i-particle pairs per thread
+__global__ void __launch_bounds__(kGThreads) k_grav_f32x2_plummer(int n, const double4 *__restrict__ src,
+                                                                  double4 *__restrict__ out, float eps2, double G) {
+  __shared__ ulonglong2 sj[kGThreads][2];
+  const int t = threadIdx.x;
+  const int i0 = blockIdx.x * kGThreads * 2 * RP;
+  const double4 anc = src[min(i0, n - 1)];
+  f32x2 xi[RP], yi[RP], zi[RP];
+  float ahi[2 * RP][4], alo[2 * RP][4];
+#pragma unroll
+  for (int p = 0; p < RP; p++) {
+    const double4 a = src[min(i0 + (2 * p) * kGThreads + t, n - 1)];
+    const double4 b = src[min(i0 + (2 * p + 1) * kGThreads + t, n - 1)];
+    xi[p] = pk2((float)(a.x - anc.x), (float)(b.x - anc.x));
+    yi[p] = pk2((float)(a.y - anc.y), (float)(b.y - anc.y));
+    zi[p] = pk2((float)(a.z - anc.z), (float)(b.z - anc.z));
+  }
+#pragma unroll
+  for (int r = 0; r < 2 * RP; r++)
+#pragma unroll
+    for (int c = 0; c < 4; c++) ahi[r][c] = alo[r][c] = 0.f;
+  const f32x2 e2 = pk2(eps2, eps2);
+  for (int j0 = 0; j0 < n; j0 += kGThreads) {
+    const int j = j0 + t;
+    __syncthreads();
+    if (j < n) {
+      const double4 q = src[j];
+      const float x = (float)(q.x - anc.x), y = (float)(q.y - anc.y), z = (float)(q.z - anc.z), m = (float)q.w;
+      sj[t][0] = make_ulonglong2(pk2(x, x), pk2(y, y));
+      sj[t][1] = make_ulonglong2(pk2(z, z), pk2(m, m));
+    } else {
+      sj[t][0] = make_ulonglong2(0ull, 0ull);
+      sj[t][1] = make_ulonglong2(0ull, 0ull);
+    }
+    __syncthreads();
+    f32x2 px[RP], py[RP], pz[RP], pp[RP];
+#pragma unroll
+    for (int p = 0; p < RP; p++) px[p] = py[p] = pz[p] = pp[p] = 0ull;
+#pragma unroll 4
+    for (int k = 0; k < kGThreads; k++) {
+      const ulonglong2 a = sj[k][0], b = sj[k][1];
+#pragma unroll
+      for (int p = 0; p < RP; p++) {
+        const f32x2 dx = sub2(a.x, xi[p]), dy = sub2(a.y, yi[p]), dz = sub2(b.x, zi[p]);
+        f32x2 r2 = fma2(dx, dx, e2);
+        r2 = fma2(dy, dy, r2);
+        r2 = fma2(dz, dz, r2);
+        float r2a, r2b;
+        upk2(r2, r2a, r2b);
+        const f32x2 inv = pk2(rsqrt_f32(r2a), rsqrt_f32(r2b));
+        const f32x2 inv2 = mul2(inv, inv);
+        const f32x2 s = mul2(b.y, inv);
+        const f32x2 s3 = mul2(s, inv2);
+        px[p] = fma2(dx, s3, px[p]);
+        py[p] = fma2(dy, s3, py[p]);
+        pz[p] = fma2(dz, s3, pz[p]);
+        pp[p] = sub2(pp[p], s);
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < RP; p++) {
+      float a0, a1;
+      upk2(px[p], a0, a1);
+      kahan_add(ahi[2 * p][0], alo[2 * p][0], a0);
+      kahan_add(ahi[2 * p + 1][0], alo[2 * p + 1][0], a1);
+      upk2(py[p], a0, a1);
+      kahan_add(ahi[2 * p][1], alo[2 * p][1], a0);
+      kahan_add(ahi[2 * p + 1][1], alo[2 * p + 1][1], a1);
+      upk2(pz[p], a0, a1);
+      kahan_add(ahi[2 * p][2], alo[2 * p][2], a0);
+      kahan_add(ahi[2 * p + 1][2], alo[2 * p + 1][2], a1);
+      upk2(pp[p], a0, a1);
+      kahan_add(ahi[2 * p][3], alo[2 * p][3], a0);
+      kahan_add(ahi[2 * p + 1][3], alo[2 * p + 1][3], a1);
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 2 * RP; r++) {
+    const int i = i0 + r * kGThreads + t;
+    if (i < n)
+      out[i] = make_double4(G * ((double)ahi[r][0] + (double)alo[r][0]), G * ((double)ahi[r][1] + (double)alo[r][1]),
+                            G * ((double)ahi[r][2] + (double)alo[r][2]), G * ((double)ahi[r][3] + (double)alo[r][3]));
+  }
+}
+
 // src = {x, y, z, m} per particle; h2src = range^2 (spline mode only)
 int launch_gravity(int n, const double4 *src, const double *h2src, double4 *out, int soft_mode, double eps, double G,
                    int precision, cudaStream_t st) {
@@ -308,7 +429,7 @@ int launch_gravity(int n, const double4 *src, const double *h2src, double4 *out,
     constexpr int R = 4;
     const int blocks = (n + kGThreads * R - 1) / (kGThreads * R);
     if (soft_mode == SPH_SOFT_PLUMMER)
-      k_grav_f32<SPH_SOFT_PLUMMER, R><<<blocks, kGThreads, 0, st>>>(n, src, h2src, out, (float)eps2, G);
+      k_grav_f32x2_plummer<R / 2><<<blocks, kGThreads, 0, st>>>(n, src, out, (float)eps2, G);
     else
       k_grav_f32<SPH_SOFT_SPLINE, R><<<blocks, kGThreads, 0, st>>>(n, src, h2src, out, (float)eps2, G);
   }

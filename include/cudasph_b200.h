@@ -72,6 +72,8 @@ typedef struct {
   int precision;     /* sph_precision */
   int ngb_cap;       /* neighbour-list capacity per particle (0 = 4 * n_target + 32) */
   int sort_every;    /* Morton re-sort period in steps (reference: 100, step.cpp:26) */
+  int mixed_sph;     /* mixed form only: bit 0 = density pair terms in FP32, bit 1 = hydro
+                        pair terms in FP32 (default 3); a cleared bit keeps that loop in FP64 */
 } sph_params;
 
 /* particle fields, addressed in the caller's ORIGINAL particle order */
@@ -184,6 +186,7 @@ size_t cudasph_sort_scratch_bytes(int n);
 int cudasph_morton_keys(int n, const double *x, const double *y, const double *z, uint64_t *keys,
                         double *box4 /* device, 4 doubles: lo xyz, scale */, void *stream);
 int cudasph_radix_sort_u64(int n, uint64_t *keys, uint32_t *vals, void *scratch, void *stream);
+
 
 /* direct-N gravity of n sources on themselves: pos4 = {x,y,z,m}, range =
  * smoothing ranges (spline mode), out4 = {gx,gy,gz,phi}; double buffers. */
