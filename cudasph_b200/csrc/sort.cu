@@ -9,6 +9,7 @@
 // warp ranks equal digits with __match_any_sync.  Ties keep their input
 // order, so with values = slot indices the permutation equals a stable sort.
 #include <cub/block/block_scan.cuh>
+#include <cstdio>
 
 #include "common.cuh"
 
@@ -220,7 +221,68 @@ int morton_keys(int n, const double4 *pos, const double *x, const double *y, con
   return 3;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the radix sort.  Its scratch (ping-pong key and
+// value buffers plus the per-block digit histograms) is a file-scope device
+// array sized for kNoAllocMaxKeys keys; every GPU that loads this library
+// holds those bytes until the process exits.
+// ---------------------------------------------------------------------------
+constexpr int kNoAllocMaxKeys = CUDASPH_SORT_NOALLOC_MAX_KEYS;
+static_assert(kNoAllocMaxKeys == (1 << 18), "header and library disagree");
+constexpr size_t round256(size_t b) { return (b + 255) / 256 * 256; }
+constexpr size_t kNoAllocScratchBytes =
+    round256((size_t)kNoAllocMaxKeys * 8) + round256((size_t)kNoAllocMaxKeys * 4) +
+    round256(256 * (((size_t)kNoAllocMaxKeys + kRadixChunk - 1) / kRadixChunk) * 4);
+
+static __device__ __align__(256) unsigned char g_noalloc_sort_scratch[kNoAllocScratchBytes];
+
 }  // namespace sph
+
+#include <mutex>
+
+namespace {
+// Host code cannot use the array's name as a device address (on the host it
+// names a stand-in object), so the address is looked up once per device with
+// that device current and cached.
+constexpr int kMaxDevices = 128;
+std::mutex g_noalloc_mu;
+void *g_noalloc_ptr[kMaxDevices] = {};
+
+int noalloc_scratch(void **out) {
+  int dev = 0;
+  SPH_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return SPH_ERR_ARG;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void *p = nullptr;
+    SPH_CUDA_TRY(cudaGetSymbolAddress(&p, sph::g_noalloc_sort_scratch));
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return SPH_OK;
+}
+}  // namespace
+
+extern "C" int cudasph_radix_sort_u64_noalloc(int n, uint64_t *keys, uint32_t *vals, void *stream) {
+  if (n < 0 || n > sph::kNoAllocMaxKeys) {
+    char msg[160];
+    snprintf(msg, sizeof(msg), "cudasph_radix_sort_u64_noalloc: n = %d outside [0, %d], the size of its fixed scratch",
+             n, sph::kNoAllocMaxKeys);
+    sph_internal_set_error(msg);
+    return SPH_ERR_ARG;
+  }
+  if (n > 0 && (!keys || !vals)) return SPH_ERR_ARG;
+  if (n <= 1) return SPH_OK;
+  void *scratch = nullptr;
+  int rc = noalloc_scratch(&scratch);
+  if (rc) return rc;
+  // nothing in the scratch has to start at zero: every pass rewrites all
+  // histogram entries and every key/value slot it later reads
+  sph::radix_sort_u64(n, keys, vals, scratch, (cudaStream_t)stream);
+  SPH_CUDA_TRY(cudaGetLastError());
+  return SPH_OK;
+}
+
 
 extern "C" size_t cudasph_sort_scratch_bytes(int n) { return sph::radix_scratch_bytes(n) + 148 * 2 * 6 * 8 + 256; }
 

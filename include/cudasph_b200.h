@@ -187,6 +187,24 @@ int cudasph_morton_keys(int n, const double *x, const double *y, const double *z
                         double *box4 /* device, 4 doubles: lo xyz, scale */, void *stream);
 int cudasph_radix_sort_u64(int n, uint64_t *keys, uint32_t *vals, void *scratch, void *stream);
 
+/* Allocation-free variant of cudasph_radix_sort_u64; it has no counterpart
+ * in the reference.  It is for callers that cannot allocate device memory on
+ * their own: a host application whose memory manager owns the whole GPU and
+ * hands out no extra buffers, a loop that must not call cudaMalloc/cudaFree
+ * because those calls can synchronise the device, or a run whose device
+ * footprint is fixed at start-up.  The caller passes only the keys and values
+ * (device pointers, results in place, same stable order as
+ * cudasph_radix_sort_u64); the scratch is a fixed array compiled into this
+ * library, sized for at most CUDASPH_SORT_NOALLOC_MAX_KEYS keys (about 3.1 MB,
+ * held on every GPU that loads the library until the process exits).  Larger
+ * n returns SPH_ERR_ARG with a message.  No cudaMalloc, cudaFree or other
+ * allocating routine is called.  The first call on a device looks up the
+ * array's device address on that device (cudaGetSymbolAddress), so make that
+ * first call outside any stream capture.  All calls share the one array and
+ * nothing in it needs to start at zero, but calls whose GPU work overlaps
+ * (two streams, or two host threads) race on it: serialise them. */
+#define CUDASPH_SORT_NOALLOC_MAX_KEYS 262144
+int cudasph_radix_sort_u64_noalloc(int n, uint64_t *keys, uint32_t *vals, void *stream);
 
 /* direct-N gravity of n sources on themselves: pos4 = {x,y,z,m}, range =
  * smoothing ranges (spline mode), out4 = {gx,gy,gz,phi}; double buffers. */
