@@ -168,6 +168,44 @@ def traffic_from_profiles(kernel_tag: str, n: int):
     return b0 * (n / n0)
 
 
+ADJOINT_N = 65536
+ADJOINT_PARAMS = dict(n_target=50.0, eos_mode=1, soft_mode=1, eps=0.01)
+
+
+def adjoint_cost(steps=3, warmup=3):
+    """Cost of the hand-written adjoint of one step relative to the forward
+    step, on the differentiation workload: an n=3 polytrope, N = 65,536,
+    ideal gas + radiation EOS, N_ngb = 50, Plummer eps = 0.01.  Device time
+    (CUDA events) of the forward step taken with keep on vs the reverse sweep
+    (cudasph_adjoint) of the same step; a checkpointed rollout additionally
+    replays each step once before its reverse sweep."""
+    from cudasph_b200 import ics
+    from cudasph_b200.simulation import Simulation, make_params
+    ic = ics.polytrope(ADJOINT_N, n_poly=3.0, n_ngb=50.0, seed=12345 + 4, mu=0.62)
+    out = {"workload": f"n=3 polytrope, N={ADJOINT_N}, gas+radiation EOS mu=0.62, N_ngb=50, Plummer eps=0.01"}
+    for name, prec in (("fp64", 0), ("mixed", 1)):
+        sim = Simulation(ic, make_params(precision=prec, **ADJOINT_PARAMS))
+        sim.set_keep(True)
+        sim.step(warmup)
+        sim.synchronize()
+        m = ic["m"]
+        sim.reset_counters()
+        sim.set_profiling(True)
+        for _ in range(steps):
+            sim.step()
+            for k, v in (("vx", m * sim.get("vx")), ("vy", m * sim.get("vy")), ("vz", m * sim.get("vz"))):
+                sim.adjoint_set(k, v)
+            sim.adjoint()
+        ph = sim.phase_times()
+        sim.set_profiling(False)
+        fwd = sum(v[0] for k, v in ph.items() if k != "adjoint") / steps
+        adj = ph["adjoint"][0] / steps
+        out[name] = {"forward_ms": fwd, "adjoint_ms": adj, "adjoint_over_forward": adj / fwd,
+                     "replay_plus_adjoint_over_forward": (fwd + adj) / fwd, "flags": sim.device_status()}
+        sim.close()
+    return out
+
+
 def cpu_reference_sample(ic, n_grav_targets=256):
     from oracle import oracle as O
     if not O.ref_available():
@@ -275,6 +313,12 @@ def run_ours(args, rank, world):
                   "against": "FP64 GPU step (equal to the FP64 oracle to 1e-12 in the parity tests) at the "
                              "same state, first step"}
         s32.close()
+        # the same with the SPH pair loops kept in FP64 (gravity pair terms FP32)
+        s0 = Simulation(ic, make_params(**dict(kw, mixed_sph=0)), device=dev)
+        s0.step(1)
+        a0 = np.stack([s0.get(k) for k in ("ax", "ay", "az")], 1)
+        errors["rms_force_rel_sph_fp64"] = rms_rel(a0, a64)
+        s0.close()
         dms64, _, ph64, _ = time_steps(s64, args.fp64_steps, 1)
         ms64 = dms64 / args.fp64_steps
         g64ms = ph64["gravity"][0] / max(ph64["gravity"][1], 1)
@@ -283,6 +327,10 @@ def run_ours(args, rank, world):
                        "gravity_ms": g64ms, "gravity_frac_of_fp64_peak": flops / (g64ms * 1e-3) / peak64}
         out["mixed_over_fp64"] = ms64 / ms_step
         out["errors"] = errors
+
+    # --- adjoint / forward cost (the differentiation form) --------------------------
+    if args.adjoint:
+        out["adjoint"] = adjoint_cost()
 
     # --- end to end through the C ABI with host buffers ----------------------------
     if args.e2e_steps > 0:
@@ -364,6 +412,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-grav-targets", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--no-adjoint", dest="adjoint", action="store_false")
     args = ap.parse_args()
     assert args.warmup >= 3 or args.impl == "reference" or os.environ.get("BENCH_ALLOW_SHORT_WARMUP")
 

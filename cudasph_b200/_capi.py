@@ -20,7 +20,10 @@ STATS = ("W", "T", "U", "E", "Jx", "Jy", "Jz", "Rcm_x", "Rcm_y", "Rcm_z", "Vcm_x
          "Fx", "Fy", "Fz", "Tx", "Ty", "Tz", "ngb_mean", "ngb_sigma", "ngb_min", "ngb_max", "dt_vel", "dt_eth",
          "dt", "time", "dt_old")
 PHASES = ("sort", "predict", "tree", "solve_range", "find_ngb", "density", "pressure", "hydro", "gravity", "finish",
-          "kick")
+          "kick", "adjoint")
+
+ADJ_FIELDS = ("x", "y", "z", "vx", "vy", "vz", "u", "ax", "ay", "az", "du", "rho")
+ADJ_ID = {k: i for i, k in enumerate(ADJ_FIELDS)}
 
 FLAG_NGB_OVERFLOW = 0x1
 FLAG_STACK_OVERFLOW = 0x2
@@ -88,6 +91,12 @@ def lib():
     L.cudasph_gravity_direct.argtypes = [ip, vp, vp, vp, ip, dp, dp, ip, vp]
     L.cudasph_fma_peak.argtypes = [ip, ip, vp]
     L.cudasph_fma_peak.restype = C.c_double
+    L.cudasph_set_keep.argtypes = [vp, ip]
+    L.cudasph_adjoint_set_field.argtypes = [vp, ip, vp, ip]
+    L.cudasph_adjoint_get_field.argtypes = [vp, ip, vp, ip]
+    L.cudasph_adjoint_set_dt.argtypes = [vp, dp]
+    L.cudasph_adjoint_get_dt.argtypes = [vp, C.POINTER(dp)]
+    L.cudasph_adjoint.argtypes = [vp]
     _lib = L
     return L
 

@@ -1,0 +1,768 @@
+// adjoint.cu -- hand-written discrete adjoint of one step.
+//
+// Forward step (step.cpp:13-147, as run by capi.cu):
+//   x1 = x0 + v0 dt0;  vp = v0 + a0 dt0/2;  up = u0 + du0 dt0/2
+//   w  = root of F_i(w) = sum_j ig(2 r_ij / w_i) - N      (h solve)
+//   rho, div, curl, omega, psi = DENSITY(x1, vp, w)
+//   P  = EOS(rho, up)
+//   ah, du1, vsig = HYDRO(x1, vp, w, rho, P, div, curl, omega, psi)
+//   a1 = ah + GRAVITY(x1)                                  (Plummer)
+//   dt1 = min_i tau_i(w, vsig, up, du1)                    (compute_timestep)
+//   v1 = v0 + a1 (dt1/2 + dt0/2);  u1 = u0 + du1 (dt1/2 + dt0/2)
+//
+// Given adjoints of (x1, v1, u1, a1, du1, dt1) and of the step's density,
+// the kernels below run the reverse sweep and leave the adjoints of
+// (x0, v0, u0, a0, du0, dt0).  The forward neighbour lists are reused; the h
+// solve enters through its implicit derivative dw_i/dx = -(dF_i/dx)/(dF_i/dw_i);
+// min (timestep) and max (signal speed) pass their adjoint to the arg-min /
+// arg-max.  The pair reverse sweeps are written out by hand with the analytic
+// derivatives of the M4 kernel family.  The SPH part is FP64; the gravity VJP
+// has an FP64 and a mixed (FP32 pair terms on anchors) form.
+#include <cstdio>
+
+#include "common.cuh"
+#include "sph_math.cuh"
+
+namespace sph {
+
+// ---------------------------------------------------------------------------
+// derivatives of the kernel functions, d/du
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double kd_dw(double u) {
+  const double ipi = 0.318309886183791;
+  if (u < 1) return 2.25 * ipi;
+  if (u < 2) return 0.75 * ipi * (4 - u * u) / (u * u);
+  return 0;
+}
+__device__ __forceinline__ double kd_dig(double u) {
+  const double c = 256.0 * 3.141592653589793;
+  if (u <= 0) return 0;
+  if (u < 1) return c * (k_w<double>(4 * u) + 16 * u * u * k_dw<double>(4 * u));
+  if (u < 2) {
+    const double s = 2 - u;
+    return c * (2 * s * k_w<double>(4 * s) / u + 16 * s * s * s * k_dw<double>(4 * s) / u +
+                s * s * k_w<double>(4 * s) / (u * u));
+  }
+  return 0;
+}
+__device__ __forceinline__ double kd_dwdh(double u) {
+  const double ipi = 0.318309886183791;
+  if (u < 1) return ipi * (15 * u - 13.5 * u * u);
+  if (u < 2) return ipi * (12 - 15 * u + 4.5 * u * u);
+  return 0;
+}
+__device__ __forceinline__ double kd_dphidh(double u) {
+  if (u < 1) return -4 * u + 6 * u * u * u - 3 * u * u * u * u;
+  if (u < 2) return -8 * u + 12 * u * u - 6 * u * u * u + u * u * u * u;
+  return 0;
+}
+__device__ __forceinline__ double kd_digdh(double u) { return 2 * u * k_dig<double>(u) + u * u * kd_dig(u); }
+
+// AdjArgs: see common.cuh
+
+
+constexpr int kAT = 256;  // threads of the per-particle kernels
+
+__device__ __forceinline__ int warp_max_i(int v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+__device__ __forceinline__ void atomic_add3(double4 *p, double x, double y, double z) {
+  atomicAdd(&p->x, x);
+  atomicAdd(&p->y, y);
+  atomicAdd(&p->z, z);
+}
+
+// -- 1. vp, up of the forward predictor; clear the internal adjoints ---------
+__global__ void k_adj_init(AdjArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  const double dth = 0.5 * a.sc[0];
+  const double4 o = a.old[i], ac = a.pre_acc[i];
+  a.vpup[i] = make_double4(o.x + ac.x * dth, o.y + ac.y * dth, o.z + ac.z * dth, o.w + ac.w * dth);
+  a.vpb[i] = make_double4(0, 0, 0, 0);
+  a.rhob[i] = a.rho_ext ? a.rho_ext[i] : 0.0;
+  a.Pb[i] = 0; a.omb[i] = 0; a.psib[i] = 0; a.divb[i] = 0; a.curlb[i] = 0;
+  a.cb[i] = 0; a.bb[i] = 0; a.prb[i] = 0;
+  a.xb[i].w = 0;  // wbar of this step starts at zero
+}
+
+// -- 2. kick adjoint + the reduction sum(vbar.a1 + ubar du1) -----------------
+__global__ void __launch_bounds__(kAT) k_adj_kick(AdjArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double s = 0;
+  if (i < a.n) {
+    const double f = 0.5 * a.sc[1] + 0.5 * a.sc[0];
+    const double4 vb = a.vb[i], d = a.dots[i];
+    double4 ab = a.ab[i];
+    ab.x += vb.x * f; ab.y += vb.y * f; ab.z += vb.z * f; ab.w += vb.w * f;
+    a.ab[i] = ab;
+    s = vb.x * d.x + vb.y * d.y + vb.z * d.z + vb.w * d.w;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  __shared__ double ws[kAT / 32];
+  if (lane_id() == 0) ws[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int k = 0; k < kAT / 32; k++) t += ws[k];
+    a.part[blockIdx.x] = t;
+  }
+}
+
+// tau_i of compute_timestep.cpp:10-16
+__device__ __forceinline__ double tau_of(double w, double vs, double up, double du, double cn1, double cn2) {
+  const double dtv = cn1 * fabs(w / vs);
+  const double dte = cn2 * fabs(up / du);
+  return 1.0 / (1.0 / dtv + 1.0 / dte);
+}
+
+// -- 3. arg-min of tau over particles (block partials) -----------------------
+__global__ void __launch_bounds__(kAT) k_adj_argmin(AdjArgs a) {
+  double t = 1e300;
+  int idx = 0x7fffffff;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+    const double ti = tau_of(a.pos[i].w, a.vsig[i], a.vpup[i].w, a.dots[i].w, a.cn1, a.cn2);
+    if (ti < t || (ti == t && i < idx)) { t = ti; idx = i; }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double t2 = __shfl_xor_sync(0xffffffffu, t, o);
+    const int i2 = __shfl_xor_sync(0xffffffffu, idx, o);
+    if (t2 < t || (t2 == t && i2 < idx)) { t = t2; idx = i2; }
+  }
+  __shared__ double st[kAT / 32];
+  __shared__ int si[kAT / 32];
+  if (lane_id() == 0) { st[threadIdx.x >> 5] = t; si[threadIdx.x >> 5] = idx; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < kAT / 32; k++)
+      if (st[k] < t || (st[k] == t && si[k] < idx)) { t = st[k]; idx = si[k]; }
+    a.part[2 * blockIdx.x] = t;
+    a.part[2 * blockIdx.x + 1] = (double)idx;
+  }
+}
+
+// -- 4. fold: dtbar, the arg-min particle, the timestep adjoint --------------
+__global__ void k_adj_timestep(AdjArgs a, int nb_kick, int nb_min) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double f = 0;
+  for (int b = 0; b < nb_kick; b++) f += a.part[b];
+  double t = 1e300;
+  int idx = 0;
+  for (int b = 0; b < nb_min; b++) {
+    const double tb = a.part[nb_kick + 2 * b];
+    const int ib = (int)a.part[nb_kick + 2 * b + 1];
+    if (tb < t || (tb == t && ib < idx)) { t = tb; idx = ib; }
+  }
+  const double dtb1 = a.asc[0] + 0.5 * f;
+  a.asc[1] = 0.5 * f;  // dtbar0 so far (predictor terms follow)
+  a.asc[3] = (double)idx;
+  a.asc[2] = 0;
+  if (dtb1 == 0 || idx >= a.n) return;
+  // tau = 1/(1/dtv + 1/dte); dtv = cn1 |w/vs|; dte = cn2 |up/du|
+  const double w = a.pos[idx].w, vs = a.vsig[idx], up = a.vpup[idx].w, du = a.dots[idx].w;
+  const double dtv = a.cn1 * fabs(w / vs), dte = a.cn2 * fabs(up / du);
+  const double tau = 1.0 / (1.0 / dtv + 1.0 / dte);
+  const double gv = isfinite(dtv) ? dtb1 * tau * tau / (dtv * dtv) : 0.0;  // dL/d dtv
+  const double ge = isfinite(dte) ? dtb1 * tau * tau / (dte * dte) : 0.0;  // dL/d dte
+  const double sw = (w / vs) >= 0 ? 1.0 : -1.0, se = (up / du) >= 0 ? 1.0 : -1.0;
+  a.xb[idx].w += gv * a.cn1 * sw / vs;
+  a.asc[2] = -gv * a.cn1 * sw * w / (vs * vs);
+  a.vpb[idx].w += ge * a.cn2 * se / du;
+  a.ab[idx].w += -ge * a.cn2 * se * up / (du * du);
+}
+
+// -- 5. gravity VJP: xbar_i += sum_j T_ij (m_i gbar_j - m_j gbar_i) ----------
+// T_ij = I / s^3 - 3 d d^T / s^5, d = x_j - x_i, s^2 = |d|^2 + eps^2 (Plummer).
+constexpr int kGA = 128;
+
+__device__ __forceinline__ double rsqrt_f64_adj(double x) {
+  double y0;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y0) : "d"(x));
+  const double e = fma(-x, y0 * y0, 1.0);
+  return fma(y0 * e, fma(0.375, e, 0.5), y0);
+}
+
+__global__ void __launch_bounds__(kGA) k_adj_grav_f64(int n, const double4 *__restrict__ src,
+                                                      const double4 *__restrict__ ab, double4 *__restrict__ xb,
+                                                      double eps2, double G) {
+  __shared__ double4 sp[kGA];
+  __shared__ double4 sg[kGA];
+  const int t = threadIdx.x;
+  const int i = blockIdx.x * kGA + t;
+  const int ii = min(i, n - 1);
+  const double4 pi = src[ii];
+  const double4 gi4 = ab[ii];
+  const double mi = pi.w, gix = gi4.x, giy = gi4.y, giz = gi4.z;
+  double rx = 0, ry = 0, rz = 0;
+  for (int j0 = 0; j0 < n; j0 += kGA) {
+    const int j = j0 + t;
+    __syncthreads();
+    if (j < n) {
+      sp[t] = src[j];
+      const double4 g = ab[j];
+      sg[t] = make_double4(g.x, g.y, g.z, 0);
+    } else {
+      sp[t] = make_double4(pi.x, pi.y, pi.z, 0);
+      sg[t] = make_double4(0, 0, 0, 0);
+    }
+    __syncthreads();
+    const int m = min(kGA, n - j0);
+    for (int k = 0; k < m; k++) {
+      const double4 q = sp[k];
+      const double4 gj = sg[k];
+      const double dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
+      const double s2 = fma(dz, dz, fma(dy, dy, fma(dx, dx, eps2)));
+      const double inv = rsqrt_f64_adj(s2);
+      const double inv2 = inv * inv, inv3 = inv2 * inv;
+      const double wx = mi * gj.x - q.w * gix, wy = mi * gj.y - q.w * giy, wz = mi * gj.z - q.w * giz;
+      const double dw = dx * wx + dy * wy + dz * wz;
+      const double c = 3.0 * inv2 * dw;
+      rx = fma(inv3, wx - c * dx, rx);
+      ry = fma(inv3, wy - c * dy, ry);
+      rz = fma(inv3, wz - c * dz, rz);
+    }
+  }
+  if (i < n) {
+    double4 x = xb[i];
+    x.x += G * rx; x.y += G * ry; x.z += G * rz;
+    xb[i] = x;
+  }
+}
+
+// mixed form of the gravity VJP: FP32 pair terms relative to the block's FP64
+// anchor, FP64 per-tile accumulation
+__global__ void __launch_bounds__(kGA) k_adj_grav_f32(int n, const double4 *__restrict__ src,
+                                                      const double4 *__restrict__ ab, double4 *__restrict__ xb,
+                                                      float eps2, double G) {
+  __shared__ float4 sp[kGA];
+  __shared__ float4 sg[kGA];
+  const int t = threadIdx.x;
+  const int i = blockIdx.x * kGA + t;
+  const int ii = min(i, n - 1);
+  const double4 anc = src[min(blockIdx.x * kGA, n - 1)];
+  const double4 pi = src[ii];
+  const double4 gi4 = ab[ii];
+  const float xi = (float)(pi.x - anc.x), yi = (float)(pi.y - anc.y), zi = (float)(pi.z - anc.z);
+  const float mi = (float)pi.w, gix = (float)gi4.x, giy = (float)gi4.y, giz = (float)gi4.z;
+  double rx = 0, ry = 0, rz = 0;
+  for (int j0 = 0; j0 < n; j0 += kGA) {
+    const int j = j0 + t;
+    __syncthreads();
+    if (j < n) {
+      const double4 q = src[j];
+      const double4 g = ab[j];
+      sp[t] = make_float4((float)(q.x - anc.x), (float)(q.y - anc.y), (float)(q.z - anc.z), (float)q.w);
+      sg[t] = make_float4((float)g.x, (float)g.y, (float)g.z, 0.f);
+    } else {
+      sp[t] = make_float4(xi, yi, zi, 0.f);
+      sg[t] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    __syncthreads();
+    float px = 0.f, py = 0.f, pz = 0.f;
+    const int m = min(kGA, n - j0);
+    for (int k = 0; k < m; k++) {
+      const float4 q = sp[k];
+      const float4 gj = sg[k];
+      const float dx = q.x - xi, dy = q.y - yi, dz = q.z - zi;
+      const float s2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
+      const float inv = rsqrtf(s2);
+      const float inv2 = inv * inv, inv3 = inv2 * inv;
+      const float wx = mi * gj.x - q.w * gix, wy = mi * gj.y - q.w * giy, wz = mi * gj.z - q.w * giz;
+      const float c = 3.f * inv2 * (dx * wx + dy * wy + dz * wz);
+      px = fmaf(inv3, wx - c * dx, px);
+      py = fmaf(inv3, wy - c * dy, py);
+      pz = fmaf(inv3, wz - c * dz, pz);
+    }
+    rx += px; ry += py; rz += pz;
+  }
+  if (i < n) {
+    double4 x = xb[i];
+    x.x += G * rx; x.y += G * ry; x.z += G * rz;
+    xb[i] = x;
+  }
+}
+
+// -- 6. hydro VJP (warp per leaf, lane per particle, lists of find_ngb) ------
+// Per pair the forward computes (dev_hydro_dots.cu:25-84 with the j-side):
+//   a_i -= m_j acc d,  a_j += m_i acc d,  du_i += ud * drdv
+// with d = x_i - x_j, ds = |d|, u = ds / h_i, h_i = w_i / 2,
+//   visc = (pr_i + pr_j)(-alpha mu + beta mu^2), mu = drdv (b_i + b_j) / ((c_i + c_j) ds)   [drdv < 0]
+//   acc = (pr_i + visc/2) dw(u) / h^5 - (pr_i om_i + psi_i/2) / m_j dig(u) / h^2
+//   ud  = m_j (pr_i + visc/2) dw(u) / h^5 - pr_i om_i dig(u) / h^2
+// where pr = P / rho^2, c = sqrt(gamma P / rho), b = Balsara factor.  The
+// reverse sweep leaves xbar, vpbar, wbar_i and the adjoints of the
+// per-particle pr, c, b, om, psi (folded into rho, P, div, curl, w later).
+__global__ void __launch_bounds__(128) k_adj_hydro(AdjArgs a) {
+  const int leaf = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (leaf >= a.nleaf) return;
+  const int lane = (int)lane_id();
+  const int s = leaf * kLeaf + lane;
+  const bool valid = s < a.n;
+  double4 pi = make_double4(0, 0, 0, 1), vi = make_double4(0, 0, 0, 0), hi4 = make_double4(1, 0, 0, 0),
+          di = make_double4(0, 0, 0, 0), abi = make_double4(0, 0, 0, 0);
+  double mi = 1;
+  int cnt = 0;
+  if (valid) {
+    pi = a.pos[s];
+    vi = a.vpup[s];
+    hi4 = a.hyd[s];
+    di = a.dd[s];
+    abi = a.ab[s];
+    mi = a.vel[s].w;
+    cnt = min(a.n_ngb[s], a.cap);
+  }
+  const int kmax = warp_max_i(cnt);
+  const int *lst = a.list + (size_t)leaf * a.cap * kLeaf + lane;
+  const double gam = a.gamma, alpha = a.alpha, beta = a.beta;
+  const double wi = pi.w, hh = 0.5 * wi;
+  const double ih = hh > 0 ? 1.0 / hh : 0.0, ih2 = ih * ih, ih5 = ih2 * ih2 * ih;
+  const double pr_i = hi4.x > 0 ? hi4.y / (hi4.x * hi4.x) : 0.0;
+  const double c_i = hi4.x > 0 ? sqrt(gam * hi4.y / hi4.x) : 0.0;
+  const double ad_i = fabs(di.x);
+  const double b_i = ad_i / (ad_i + di.y + 0.0001 * c_i / (0.5 * wi));
+  const double om_i = di.z, psi_i = a.use_psi ? di.w : 0.0;
+  // i-side accumulators
+  double xbx = 0, xby = 0, xbz = 0, vbx = 0, vby = 0, vbz = 0, ihb = 0;
+  double prb_i = 0, cb_i = 0, bb_i = 0, omb_i = 0, psib_i = 0;
+  for (int k = 0; k < kmax; k++) {
+    if (k >= cnt) continue;
+    const int j = __ldg(lst + (size_t)k * kLeaf);
+    if (j == s) continue;
+    const double4 pj = ld4(a.pos + j), vj = ld4(a.vpup + j), hj = ld4(a.hyd + j), dj = ld4(a.dd + j);
+    const double4 abj = ld4(a.ab + j);
+    const double mj = __ldg(&a.vel[j].w);
+    const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+    const double dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
+    const double ds = sqrt(dx * dx + dy * dy + dz * dz);
+    const double drdv = dx * dvx + dy * dvy + dz * dvz;
+    const double u = ds * ih;
+    const double pr_j = hj.y / (hj.x * hj.x);
+    const double c_j = sqrt(gam * hj.y / hj.x);
+    const double ad_j = fabs(dj.x);
+    const double b_j = ad_j / (ad_j + dj.y + 0.0001 * c_j / (0.5 * pj.w));
+    // forward
+    const bool neg = drdv < 0;
+    const double S = c_i + c_j, B = b_i + b_j, Q = pr_i + pr_j;
+    double mu0 = 0, mu = 0, visc = 0;
+    if (neg) {
+      mu0 = drdv / (S * ds);
+      mu = mu0 * B;
+      visc = Q * (-alpha * mu + beta * mu * mu);
+    }
+    const double dwu = k_dw<double>(u), digu = k_dig<double>(u);
+    const double A1 = pr_i + 0.5 * visc;
+    const double K2 = pr_i * om_i + 0.5 * psi_i;
+    const double acc = A1 * dwu * ih5 - K2 / mj * digu * ih2;
+    const double ud = mj * A1 * dwu * ih5 - pr_i * om_i * digu * ih2;
+    // output adjoints of the pair: force vector acc*d (i: -m_j, j: +m_i), and ud*drdv
+    const double gx = -mj * abi.x + mi * abj.x, gy = -mj * abi.y + mi * abj.y, gz = -mj * abi.z + mi * abj.z;
+    const double accb = gx * dx + gy * dy + gz * dz;
+    const double udb = abi.w * drdv;
+    double dxb = acc * gx, dyb = acc * gy, dzb = acc * gz;
+    double drdvb = abi.w * ud;
+    // acc, ud -> A1, dwu, digu, ih5, ih2, pr_i, om_i, psi_i
+    const double A1b = accb * dwu * ih5 + udb * mj * dwu * ih5;
+    const double dwub = accb * A1 * ih5 + udb * mj * A1 * ih5;
+    const double digub = -accb * K2 / mj * ih2 - udb * pr_i * om_i * ih2;
+    const double ih5b = accb * A1 * dwu + udb * mj * A1 * dwu;
+    const double ih2b = -accb * K2 / mj * digu - udb * pr_i * om_i * digu;
+    const double K2b = -accb / mj * digu * ih2;
+    prb_i += K2b * om_i - udb * om_i * digu * ih2 + A1b;
+    omb_i += K2b * pr_i - udb * pr_i * digu * ih2;
+    psib_i += 0.5 * K2b;
+    ihb += ih5b * 5.0 * ih2 * ih2 + ih2b * 2.0 * ih;
+    // visc
+    if (neg) {
+      const double viscb = 0.5 * A1b;
+      const double Qb = viscb * (-alpha * mu + beta * mu * mu);
+      const double mub = viscb * Q * (-alpha + 2.0 * beta * mu);
+      prb_i += Qb;
+      const double prjb = Qb;
+      const double mu0b = mub * B;
+      const double Bb = mub * mu0;
+      bb_i += Bb;
+      const double Sb = -mu0b * mu0 / S;
+      cb_i += Sb;
+      drdvb += mu0b / (S * ds);
+      const double dsb_v = -mu0b * mu0 / ds;
+      atomicAdd(&a.prb[j], prjb);
+      atomicAdd(&a.bb[j], Bb);
+      atomicAdd(&a.cb[j], Sb);
+      if (ds > 0) {
+        dxb += dsb_v * dx / ds; dyb += dsb_v * dy / ds; dzb += dsb_v * dz / ds;
+      }
+    }
+    // u = ds * ih
+    const double ub = dwub * kd_dw(u) + digub * kd_dig(u);
+    ihb += ub * ds;
+    const double dsb = ub * ih;
+    if (ds > 0) {
+      dxb += dsb * dx / ds; dyb += dsb * dy / ds; dzb += dsb * dz / ds;
+    }
+    // drdv = d . dv
+    dxb += drdvb * dvx; dyb += drdvb * dvy; dzb += drdvb * dvz;
+    const double dvxb = drdvb * dx, dvyb = drdvb * dy, dvzb = drdvb * dz;
+    xbx += dxb; xby += dyb; xbz += dzb;
+    vbx += dvxb; vby += dvyb; vbz += dvzb;
+    atomic_add3(&a.xb[j], -dxb, -dyb, -dzb);
+    atomic_add3(&a.vpb[j], -dvxb, -dvyb, -dvzb);
+  }
+  if (!valid) return;
+  atomic_add3(&a.xb[s], xbx, xby, xbz);
+  atomic_add3(&a.vpb[s], vbx, vby, vbz);
+  // ih = 2 / w  ->  wbar += ihb * (-2 / w^2) = -ihb ih^2 / 2
+  atomicAdd(&a.xb[s].w, -0.5 * ihb * ih * ih);
+  atomicAdd(&a.prb[s], prb_i);
+  atomicAdd(&a.cb[s], cb_i);
+  atomicAdd(&a.bb[s], bb_i);
+  atomicAdd(&a.omb[s], omb_i);
+  atomicAdd(&a.psib[s], a.use_psi ? psib_i : 0.0);
+}
+
+// -- 7. signal-speed adjoint at the arg-min particle of the timestep ---------
+// vsig_i = max_j vs_ij, vs = c_i + c_j - beta drdv / ds (drdv < 0) else c_i + c_j;
+// the adjoint goes to the first pair (list order) that attains the maximum.
+__global__ void k_adj_vsig(AdjArgs a) {
+  if (threadIdx.x != 0) return;
+  const double vsb = a.asc[2];
+  const int s = (int)a.asc[3];
+  if (vsb == 0 || s < 0 || s >= a.n) return;
+  const int leaf = s / kLeaf, lane = s % kLeaf;
+  const int cnt = min(a.n_ngb[s], a.cap);
+  const double4 pi = a.pos[s], vi = a.vpup[s], hi4 = a.hyd[s];
+  const double gam = a.gamma, beta = a.beta;
+  const double c_i = sqrt(gam * hi4.y / hi4.x);
+  const double target = a.vsig[s];
+  for (int k = 0; k < cnt; k++) {
+    const int j = a.list[((size_t)leaf * a.cap + k) * kLeaf + lane];
+    const double4 pj = a.pos[j], vj = a.vpup[j], hj = a.hyd[j];
+    const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+    const double dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
+    const double ds = sqrt(dx * dx + dy * dy + dz * dz);
+    const double drdv = dx * dvx + dy * dvy + dz * dvz;
+    const double c_j = sqrt(gam * hj.y / hj.x);
+    double vs = c_i + c_j;
+    if (drdv < 0) vs -= beta * drdv / ds;
+    if (fabs(vs - target) > 1e-12 * fabs(target)) continue;
+    a.cb[s] += vsb;
+    a.cb[j] += vsb;
+    if (drdv < 0 && ds > 0) {
+      const double drdvb = -beta * vsb / ds;
+      const double dsb = beta * vsb * drdv / (ds * ds);
+      const double gx = dsb * dx / ds + drdvb * dvx, gy = dsb * dy / ds + drdvb * dvy, gz = dsb * dz / ds + drdvb * dvz;
+      a.xb[s].x += gx; a.xb[s].y += gy; a.xb[s].z += gz;
+      a.xb[j].x -= gx; a.xb[j].y -= gy; a.xb[j].z -= gz;
+      a.vpb[s].x += drdvb * dx; a.vpb[s].y += drdvb * dy; a.vpb[s].z += drdvb * dz;
+      a.vpb[j].x -= drdvb * dx; a.vpb[j].y -= drdvb * dy; a.vpb[j].z -= drdvb * dz;
+    }
+    return;
+  }
+}
+
+// -- 8. per particle: pr, c, b -> rho, P, div, curl, w; then the EOS ---------
+__global__ void k_adj_particle(AdjArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  const double4 h = a.hyd[i], d = a.dd[i], p = a.pos[i];
+  const double rho = h.x, P = h.y, w = p.w, gam = a.gamma;
+  double rhob = a.rhob[i], Pb = a.Pb[i];
+  if (!(rho > 0)) return;
+  // pr = P / rho^2
+  const double prb = a.prb[i];
+  Pb += prb / (rho * rho);
+  rhob += -2.0 * prb * P / (rho * rho * rho);
+  // c = sqrt(gamma P / rho)
+  const double c = sqrt(gam * P / rho);
+  double cb = a.cb[i];
+  // b = |D| / (|D| + C + 1e-4 c / (w/2))
+  const double bb = a.bb[i];
+  double divb = a.divb[i], curlb = a.curlb[i], wb = 0;
+  if (bb != 0) {
+    const double ad = fabs(d.x);
+    const double kk = 0.0001 / (0.5 * w);
+    const double den = ad + d.y + kk * c;
+    const double q = bb / (den * den);
+    const double adb = q * (den - ad);
+    curlb += -q * ad;
+    cb += -q * ad * kk;
+    wb += q * ad * kk * c / w;  // d(kk)/dw = -kk / w
+    divb += d.x >= 0 ? adb : -adb;
+  }
+  if (c > 0) {
+    Pb += cb * gam / (2.0 * c * rho);
+    rhob += -cb * c / (2.0 * rho);
+  }
+  // EOS: P(rho, up)
+  double upb = 0;
+  const double up = a.vpup[i].w;
+  if (a.eos_mode == SPH_EOS_IDEAL) {
+    rhob += Pb * (gam - 1) * up;
+    upb += Pb * (gam - 1) * rho;
+  } else if (Pb != 0) {
+    const double DU = 5.89994031541978, EU = 1.90698842928778e+15, PU = 1.1251117914994e+16;
+    const double AMU = 1.66054e-24, KB = 1.380658e-16, AR = 7.56591414984829e-15, tb = 1.0e6;
+    const double mu = h.w * AMU;
+    const double dens = rho * DU, en = up * EU;
+    const double r = -dens * (en / (tb * tb)) / (AR * tb * tb);
+    const double qq = (KB / AR) / (gam - 1) * dens / (((mu * tb) * tb) * tb);
+    // the positive root of x^4 + q x + r = 0 (T = tb x), recovered from P:
+    // (dens KB T / mu + AR T^4 / 3) / PU = P is solved by Newton from the bound
+    double x = fmin(-r / qq, pow(-r, 0.25));
+    for (int it = 0; it < 60; it++) {
+      const double x3 = x * x * x;
+      const double xn = x - (x3 * x + qq * x + r) / (4 * x3 + qq);
+      if (xn == x) break;
+      x = xn;
+    }
+    const double T = tb * x;
+    const double dPdT = (dens * KB / mu + 4.0 * AR * T * T * T / 3.0) / PU;
+    const double den4 = 4 * x * x * x + qq;
+    const double dxdrho = x * x * x * x / (rho * den4);    // dq/drho = q/rho, dr/drho = r/rho
+    const double dxdu = -(r / up) / den4;                   // dr/du = r/u
+    rhob += Pb * (KB * T / mu * DU / PU + dPdT * tb * dxdrho);
+    upb += Pb * dPdT * tb * dxdu;
+  }
+  a.rhob[i] = rhob;
+  a.divb[i] = divb;
+  a.curlb[i] = curlb;
+  a.vpb[i].w += upb;
+  a.xb[i].w += wb;
+}
+
+// -- 9. density VJP (warp per leaf): epilogue reverse, then pairs ------------
+// Forward (dev_density_loop.cu:29-86, with m_j in the divergence weight):
+//   R = sum m_j W(u), O = sum m_j dwdh(u), Q = sum m_j dphidh(u), S = -sum digdh(u),
+//   Dv = sum m_j dw(u) (d.dv), Cv = sum m_j dw(u) (d x dv),  u = 2 ds / w
+//   rho = R/h^3, om = O/(h^3 S), psi = Q/(h S), div = Dv/(rho h^5), curl = |Cv|/(rho h^5)
+__global__ void __launch_bounds__(128) k_adj_density(AdjArgs a) {
+  const int leaf = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (leaf >= a.nleaf) return;
+  const int lane = (int)lane_id();
+  const int s = leaf * kLeaf + lane;
+  const bool valid = s < a.n;
+  double4 pi = make_double4(0, 0, 0, 1), vi = make_double4(0, 0, 0, 0);
+  int cnt = 0;
+  if (valid) {
+    pi = a.pos[s];
+    vi = a.vpup[s];
+    cnt = min(a.n_ngb[s], a.cap);
+  }
+  const int kmax = warp_max_i(cnt);
+  const int *lst = a.list + (size_t)leaf * a.cap * kLeaf + lane;
+  const double w = pi.w;
+  const double i2w = w > 0 ? 2.0 / w : 0.0;
+  // forward sums
+  double R = 0, O = 0, Qs = 0, S = 0, Dv = 0, Cx = 0, Cy = 0, Cz = 0;
+  for (int k = 0; k < kmax; k++) {
+    if (k >= cnt) continue;
+    const int j = __ldg(lst + (size_t)k * kLeaf);
+    const double4 pj = ld4(a.pos + j), vj = ld4(a.vpup + j);
+    const double mj = __ldg(&a.vel[j].w);
+    const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+    const double dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
+    const double u = sqrt(dx * dx + dy * dy + dz * dz) * i2w;
+    R += mj * k_w<double>(u);
+    O += mj * k_dwdh<double>(u);
+    Qs += mj * k_dphidh<double>(u);
+    S -= k_digdh<double>(u);
+    const double wt = mj * k_dw<double>(u);
+    Dv += wt * (dx * dvx + dy * dvy + dz * dvz);
+    Cx += wt * (dy * dvz - dz * dvy);
+    Cy += wt * (dz * dvx - dx * dvz);
+    Cz += wt * (dx * dvy - dy * dvx);
+  }
+  // epilogue reverse
+  double Rb = 0, Ob = 0, Qb = 0, Sb = 0, Dvb = 0, Cxb = 0, Cyb = 0, Czb = 0, wb = 0;
+  if (valid && w > 0 && cnt > 0) {
+    const double h = 0.5 * w, h3 = h * h * h, h5 = h3 * h * h;
+    const double rho = R / h3;
+    const double div = Dv / (rho * h5);
+    const double cm = sqrt(Cx * Cx + Cy * Cy + Cz * Cz);
+    const double curl = cm / (rho * h5);
+    double rhob = a.rhob[s], hb = 0;
+    const double divb = a.divb[s], curlb = a.curlb[s];
+    Dvb = divb / (rho * h5);
+    rhob -= divb * div / rho;
+    hb -= 5.0 * divb * div / h;
+    if (cm > 0) {
+      const double f = curlb / (cm * rho * h5);
+      Cxb = f * Cx; Cyb = f * Cy; Czb = f * Cz;
+    }
+    rhob -= curlb * curl / rho;
+    hb -= 5.0 * curlb * curl / h;
+    if (S != 0) {
+      const double om = O / (h3 * S), ps = Qs / (h * S);
+      const double omb = a.omb[s], psb = a.psib[s];
+      Ob = omb / (h3 * S);
+      Sb -= omb * om / S;
+      hb -= 3.0 * omb * om / h;
+      Qb = psb / (h * S);
+      Sb -= psb * ps / S;
+      hb -= psb * ps / h;
+    }
+    Rb = rhob / h3;
+    hb -= 3.0 * rhob * rho / h;
+    wb = 0.5 * hb;
+  }
+  // pairs
+  double xbx = 0, xby = 0, xbz = 0, vbx = 0, vby = 0, vbz = 0;
+  for (int k = 0; k < kmax; k++) {
+    if (k >= cnt) continue;
+    const int j = __ldg(lst + (size_t)k * kLeaf);
+    if (j == s) continue;
+    const double4 pj = ld4(a.pos + j), vj = ld4(a.vpup + j);
+    const double mj = __ldg(&a.vel[j].w);
+    const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+    const double dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
+    const double ds = sqrt(dx * dx + dy * dy + dz * dz);
+    const double u = ds * i2w;
+    const double dwu = k_dw<double>(u);
+    const double drdv = dx * dvx + dy * dvy + dz * dvz;
+    const double crx = dy * dvz - dz * dvy, cry = dz * dvx - dx * dvz, crz = dx * dvy - dy * dvx;
+    const double cdot = Cxb * crx + Cyb * cry + Czb * crz;
+    const double ub = mj * (Rb * u * dwu + Ob * kd_dwdh(u) + Qb * kd_dphidh(u)) - Sb * kd_digdh(u) +
+                      mj * kd_dw(u) * (Dvb * drdv + cdot);
+    const double wt = mj * dwu;
+    // d/d(d) of Dvb (d.dv) + Cb.(d x dv) = Dvb dv + dv x Cb ; d/d(dv) = Dvb d + Cb x d
+    double dxb = wt * (Dvb * dvx + (dvy * Czb - dvz * Cyb));
+    double dyb = wt * (Dvb * dvy + (dvz * Cxb - dvx * Czb));
+    double dzb = wt * (Dvb * dvz + (dvx * Cyb - dvy * Cxb));
+    const double dvxb = wt * (Dvb * dx + (Cyb * dz - Czb * dy));
+    const double dvyb = wt * (Dvb * dy + (Czb * dx - Cxb * dz));
+    const double dvzb = wt * (Dvb * dz + (Cxb * dy - Cyb * dx));
+    if (ds > 0) {
+      const double g = ub * i2w / ds;
+      dxb += g * dx; dyb += g * dy; dzb += g * dz;
+    }
+    wb -= ub * u / w;
+    xbx += dxb; xby += dyb; xbz += dzb;
+    vbx += dvxb; vby += dvyb; vbz += dvzb;
+    atomic_add3(&a.xb[j], -dxb, -dyb, -dzb);
+    atomic_add3(&a.vpb[j], -dvxb, -dvyb, -dvzb);
+  }
+  if (!valid) return;
+  atomic_add3(&a.xb[s], xbx, xby, xbz);
+  atomic_add3(&a.vpb[s], vbx, vby, vbz);
+  atomicAdd(&a.xb[s].w, wb);
+}
+
+// -- 10. h-solve implicit derivative: xbar -= lambda_i dF_i/dx, lambda_i = wbar_i / F_w,i
+// F_i = sum_j ig(2 ds/w_i) - N;  F_w = -(1/w) sum digdh(u);  dF_i/dx_i = sum_j 4 dig(u)/w^2 d_ij
+__global__ void __launch_bounds__(128) k_adj_hsolve(AdjArgs a) {
+  const int leaf = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (leaf >= a.nleaf) return;
+  const int lane = (int)lane_id();
+  const int s = leaf * kLeaf + lane;
+  const bool valid = s < a.n;
+  double4 pi = make_double4(0, 0, 0, 1);
+  int cnt = 0;
+  double wbar = 0;
+  if (valid) {
+    pi = a.pos[s];
+    cnt = min(a.n_ngb[s], a.cap);
+    wbar = a.xb[s].w;
+  }
+  const int kmax = warp_max_i(cnt);
+  const int *lst = a.list + (size_t)leaf * a.cap * kLeaf + lane;
+  const double w = pi.w;
+  const double i2w = w > 0 ? 2.0 / w : 0.0;
+  double Fw = 0;
+  for (int k = 0; k < kmax; k++) {
+    if (k >= cnt) continue;
+    const int j = __ldg(lst + (size_t)k * kLeaf);
+    const double4 pj = ld4(a.pos + j);
+    const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+    Fw -= k_digdh<double>(sqrt(dx * dx + dy * dy + dz * dz) * i2w);
+  }
+  Fw = w > 0 ? Fw / w : 0.0;
+  const double lam = (valid && Fw != 0 && wbar != 0) ? wbar / Fw : 0.0;
+  double xbx = 0, xby = 0, xbz = 0;
+  if (__any_sync(0xffffffffu, lam != 0)) {
+    for (int k = 0; k < kmax; k++) {
+      if (k >= cnt || lam == 0) continue;
+      const int j = __ldg(lst + (size_t)k * kLeaf);
+      if (j == s) continue;
+      const double4 pj = ld4(a.pos + j);
+      const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+      const double u = sqrt(dx * dx + dy * dy + dz * dz) * i2w;
+      const double c = -lam * 4.0 * k_dig<double>(u) / (w * w);
+      xbx += c * dx; xby += c * dy; xbz += c * dz;
+      atomic_add3(&a.xb[j], -c * dx, -c * dy, -c * dz);
+    }
+  }
+  if (!valid) return;
+  atomic_add3(&a.xb[s], xbx, xby, xbz);
+}
+
+// -- 11. predictor reverse + dtbar0 partials ---------------------------------
+__global__ void __launch_bounds__(kAT) k_adj_predict(AdjArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double s = 0;
+  if (i < a.n) {
+    const double dt0 = a.sc[0], dth = 0.5 * dt0;
+    const double4 xb = a.xb[i], vpb = a.vpb[i], o = a.old[i], ac = a.pre_acc[i];
+    double4 vb = a.vb[i];
+    vb.x += xb.x * dt0 + vpb.x;
+    vb.y += xb.y * dt0 + vpb.y;
+    vb.z += xb.z * dt0 + vpb.z;
+    vb.w += vpb.w;
+    a.vb[i] = vb;
+    a.ab[i] = make_double4(vpb.x * dth, vpb.y * dth, vpb.z * dth, vpb.w * dth);
+    a.xb[i].w = 0;
+    s = xb.x * o.x + xb.y * o.y + xb.z * o.z + 0.5 * (vpb.x * ac.x + vpb.y * ac.y + vpb.z * ac.z + vpb.w * ac.w);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  __shared__ double ws[kAT / 32];
+  if (lane_id() == 0) ws[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int k = 0; k < kAT / 32; k++) t += ws[k];
+    a.part[blockIdx.x] = t;
+  }
+}
+
+__global__ void k_adj_predict_final(AdjArgs a, int nb) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double t = 0;
+  for (int b = 0; b < nb; b++) t += a.part[b];
+  a.asc[1] += t;
+}
+
+// block partials: nb (kick sum) + 2 nb (arg-min value, index), reused by the predictor sum
+int adjoint_part_doubles(int n) { return 3 * ((n + kAT - 1) / kAT) + 8; }
+
+// The whole reverse sweep; src = packed gravity sources {x1, m} of the step.
+int launch_adjoint(AdjArgs a, const double4 *src, double eps, double G, int precision, cudaStream_t st) {
+  const int n = a.n;
+  const int nb = (n + kAT - 1) / kAT;
+  const int warps_blocks = (a.nleaf * 32 + 127) / 128;
+  int launches = 0;
+  k_adj_init<<<nb, kAT, 0, st>>>(a); launches++;
+  k_adj_kick<<<nb, kAT, 0, st>>>(a); launches++;
+  AdjArgs b = a;
+  b.part = a.part + nb;
+  k_adj_argmin<<<nb, kAT, 0, st>>>(b); launches++;
+  k_adj_timestep<<<1, 32, 0, st>>>(a, nb, nb); launches++;
+  if (precision == SPH_PREC_FP64)
+    k_adj_grav_f64<<<(n + kGA - 1) / kGA, kGA, 0, st>>>(n, src, a.ab, a.xb, eps * eps, G);
+  else
+    k_adj_grav_f32<<<(n + kGA - 1) / kGA, kGA, 0, st>>>(n, src, a.ab, a.xb, (float)(eps * eps), G);
+  launches++;
+  k_adj_hydro<<<warps_blocks, 128, 0, st>>>(a); launches++;
+  k_adj_vsig<<<1, 32, 0, st>>>(a); launches++;
+  k_adj_particle<<<nb, kAT, 0, st>>>(a); launches++;
+  k_adj_density<<<warps_blocks, 128, 0, st>>>(a); launches++;
+  k_adj_hsolve<<<warps_blocks, 128, 0, st>>>(a); launches++;
+  k_adj_predict<<<nb, kAT, 0, st>>>(a); launches++;
+  k_adj_predict_final<<<1, 32, 0, st>>>(a, nb); launches++;
+  return launches;
+}
+
+}  // namespace sph

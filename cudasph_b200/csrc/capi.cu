@@ -44,6 +44,8 @@ int launch_invert(int n, const int *id, int *slot_of, cudaStream_t st);
 int launch_field_io(int n, double *arr, int stride, int comp, const int *id, double *flat, int to_state,
                     cudaStream_t st);
 int launch_iota(int n, int *id, cudaStream_t st);
+int adjoint_part_doubles(int n);
+int launch_adjoint(AdjArgs a, const double4 *src, double eps, double G, int precision, cudaStream_t st);
 }  // namespace sph
 
 using namespace sph;
@@ -91,6 +93,11 @@ struct sph_ctx {
   bool profiling = false;
   std::vector<cudaEvent_t> ev[SPH_NPHASES];
   std::vector<cudaEvent_t> pool;
+  // adjoint (allocated on the first cudasph_set_keep(ctx, 1))
+  bool keep = false, kept = false;
+  double4 *pre_acc = nullptr, *xb = nullptr, *vb = nullptr, *ab = nullptr, *vpb = nullptr, *vpup = nullptr;
+  double *rhob = nullptr, *Pb = nullptr, *omb = nullptr, *psib = nullptr, *divb = nullptr, *curlb = nullptr;
+  double *cb = nullptr, *bb = nullptr, *prb = nullptr, *rho_ext = nullptr, *asc = nullptr, *apart = nullptr;
 };
 
 namespace {
@@ -232,6 +239,9 @@ extern "C" int cudasph_destroy(sph_ctx *c) {
   cudaFree(c->tlo); cudaFree(c->thi); cudaFree(c->keys); cudaFree(c->vals); cudaFree(c->sort_scratch);
   cudaFree(c->bbox_part); cudaFree(c->box4); cudaFree(c->gsrc); cudaFree(c->gh2); cudaFree(c->flags);
   cudaFree(c->sc); cudaFree(c->fin_part); cudaFree(c->flat); cudaFree(c->slot_of);
+  cudaFree(c->pre_acc); cudaFree(c->xb); cudaFree(c->vb); cudaFree(c->ab); cudaFree(c->vpb); cudaFree(c->vpup);
+  cudaFree(c->rhob); cudaFree(c->Pb); cudaFree(c->omb); cudaFree(c->psib); cudaFree(c->divb); cudaFree(c->curlb);
+  cudaFree(c->cb); cudaFree(c->bb); cudaFree(c->prb); cudaFree(c->rho_ext); cudaFree(c->asc); cudaFree(c->apart);
   for (int ph = 0; ph < SPH_NPHASES; ph++)
     for (cudaEvent_t e : c->ev[ph]) cudaEventDestroy(e);
   for (cudaEvent_t e : c->pool) cudaEventDestroy(e);
@@ -636,11 +646,19 @@ extern "C" int cudasph_step(sph_ctx *c) {
   c->iteration++;
   if (c->need_sort || (c->p.sort_every > 0 && c->iteration % c->p.sort_every == 0))
     if ((rc = cudasph_sort(c))) return rc;
+  if (c->keep) {
+    // the adjoint needs the accelerations the predictor uses (a0, du0)
+    SPH_CUDA_TRY(cudaSetDevice(c->device));
+    SPH_CUDA_TRY(cudaMemcpyAsync(c->pre_acc, c->f[c->cur].dots, sizeof(double4) * c->n, cudaMemcpyDeviceToDevice,
+                                 c->st));
+  }
+  c->kept = false;
   if ((rc = cudasph_predict(c))) return rc;
   if ((rc = cudasph_sph_accelerations(c))) return rc;
   if ((rc = cudasph_gravity(c))) return rc;
   if ((rc = cudasph_finish(c))) return rc;
   if ((rc = cudasph_kick(c))) return rc;
+  c->kept = c->keep;
   return SPH_OK;
 }
 
@@ -721,6 +739,125 @@ extern "C" int cudasph_reset_counters(sph_ctx *c) {
 }
 
 extern "C" long long cudasph_kernel_launches(const sph_ctx *c) { return c ? c->launches : 0; }
+
+// ------------------------------- the adjoint --------------------------------
+extern "C" int cudasph_set_keep(sph_ctx *c, int on) {
+  if (!c) return SPH_ERR_ARG;
+  SPH_CUDA_TRY(cudaSetDevice(c->device));
+  if (on && !c->pre_acc) {
+    const int n = c->n;
+    int rc = SPH_OK;
+    double4 **d4[] = {&c->pre_acc, &c->xb, &c->vb, &c->ab, &c->vpb, &c->vpup};
+    for (double4 **p : d4)
+      if (!rc) rc = dalloc(p, n);
+    double **d1[] = {&c->rhob, &c->Pb, &c->omb, &c->psib, &c->divb, &c->curlb, &c->cb, &c->bb, &c->prb, &c->rho_ext};
+    for (double **p : d1)
+      if (!rc) rc = dalloc(p, n);
+    if (!rc) rc = dalloc(&c->asc, 8);
+    if (!rc) rc = dalloc(&c->apart, adjoint_part_doubles(n));
+    if (rc) return rc;
+    SPH_CUDA_TRY(cudaMemsetAsync(c->xb, 0, sizeof(double4) * n, c->st));
+    SPH_CUDA_TRY(cudaMemsetAsync(c->vb, 0, sizeof(double4) * n, c->st));
+    SPH_CUDA_TRY(cudaMemsetAsync(c->ab, 0, sizeof(double4) * n, c->st));
+    SPH_CUDA_TRY(cudaMemsetAsync(c->rho_ext, 0, sizeof(double) * n, c->st));
+    SPH_CUDA_TRY(cudaMemsetAsync(c->asc, 0, sizeof(double) * 8, c->st));
+  }
+  c->keep = on != 0;
+  return SPH_OK;
+}
+
+static int adj_ref(sph_ctx *c, int field, double **base, int *stride, int *comp) {
+  if (!c->pre_acc) return SPH_ERR_STATE;
+  *stride = 4;
+  if (field >= SPH_ADJ_X && field <= SPH_ADJ_Z) { *base = (double *)c->xb; *comp = field - SPH_ADJ_X; }
+  else if (field >= SPH_ADJ_VX && field <= SPH_ADJ_U) { *base = (double *)c->vb; *comp = field - SPH_ADJ_VX; }
+  else if (field >= SPH_ADJ_AX && field <= SPH_ADJ_DU) { *base = (double *)c->ab; *comp = field - SPH_ADJ_AX; }
+  else if (field == SPH_ADJ_RHO) { *base = c->rho_ext; *stride = 1; *comp = 0; }
+  else return SPH_ERR_ARG;
+  return SPH_OK;
+}
+
+extern "C" int cudasph_adjoint_set_field(sph_ctx *c, int field, const double *src, int on_device) {
+  if (!c || !src) return SPH_ERR_ARG;
+  double *base;
+  int stride, comp;
+  int rc = adj_ref(c, field, &base, &stride, &comp);
+  if (rc) return rc;
+  SPH_CUDA_TRY(cudaSetDevice(c->device));
+  rc = copy_in(c, src, sizeof(double) * c->n, on_device, c->flat);
+  if (rc) return rc;
+  launch_field_io(c->n, base, stride, comp, c->f[c->cur].id, c->flat, 1, c->st);
+  c->launches++;
+  SPH_CUDA_TRY(cudaGetLastError());
+  if (!on_device) SPH_CUDA_TRY(cudaStreamSynchronize(c->st));
+  return SPH_OK;
+}
+
+extern "C" int cudasph_adjoint_get_field(sph_ctx *c, int field, double *dst, int on_device) {
+  if (!c || !dst) return SPH_ERR_ARG;
+  double *base;
+  int stride, comp;
+  int rc = adj_ref(c, field, &base, &stride, &comp);
+  if (rc) return rc;
+  SPH_CUDA_TRY(cudaSetDevice(c->device));
+  launch_field_io(c->n, base, stride, comp, c->f[c->cur].id, c->flat, 0, c->st);
+  c->launches++;
+  SPH_CUDA_TRY(cudaMemcpyAsync(dst, c->flat, sizeof(double) * c->n,
+                               on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, c->st));
+  if (!on_device) SPH_CUDA_TRY(cudaStreamSynchronize(c->st));
+  return SPH_OK;
+}
+
+extern "C" int cudasph_adjoint_set_dt(sph_ctx *c, double dtbar) {
+  if (!c || !c->asc) return c ? SPH_ERR_STATE : SPH_ERR_ARG;
+  SPH_CUDA_TRY(cudaSetDevice(c->device));
+  SPH_CUDA_TRY(cudaMemcpyAsync(c->asc, &dtbar, sizeof(double), cudaMemcpyHostToDevice, c->st));
+  SPH_CUDA_TRY(cudaStreamSynchronize(c->st));
+  return SPH_OK;
+}
+
+extern "C" int cudasph_adjoint_get_dt(sph_ctx *c, double *dtbar) {
+  if (!c || !dtbar || !c->asc) return c ? SPH_ERR_STATE : SPH_ERR_ARG;
+  SPH_CUDA_TRY(cudaSetDevice(c->device));
+  SPH_CUDA_TRY(cudaMemcpyAsync(dtbar, c->asc + 1, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  SPH_CUDA_TRY(cudaStreamSynchronize(c->st));
+  return SPH_OK;
+}
+
+extern "C" int cudasph_adjoint(sph_ctx *c) {
+  if (!c) return SPH_ERR_ARG;
+  if (!c->kept) {
+    sph_internal_set_error("cudasph_adjoint: the last step was not taken with cudasph_set_keep(ctx, 1)");
+    return SPH_ERR_STATE;
+  }
+  if (c->p.soft_mode != SPH_SOFT_PLUMMER) {
+    sph_internal_set_error("cudasph_adjoint: implemented for Plummer softening");
+    return SPH_ERR_ARG;
+  }
+  SPH_CUDA_TRY(cudaSetDevice(c->device));
+  Fields &F = c->f[c->cur];
+  AdjArgs a;
+  memset(&a, 0, sizeof(a));
+  a.n = c->n;
+  a.nleaf = c->tree.count[0];
+  a.cap = c->list_cap;
+  a.pos = F.pos; a.vel = F.vel; a.hyd = F.hyd; a.dd = F.dd; a.dots = F.dots; a.vsig = F.vsig;
+  a.old = c->old; a.pre_acc = c->pre_acc; a.x0 = nullptr; a.vpup = c->vpup;
+  a.n_ngb = c->n_ngb; a.list = c->list; a.sc = c->sc;
+  a.xb = c->xb; a.vb = c->vb; a.ab = c->ab; a.vpb = c->vpb;
+  a.rhob = c->rhob; a.Pb = c->Pb; a.omb = c->omb; a.psib = c->psib; a.divb = c->divb; a.curlb = c->curlb;
+  a.cb = c->cb; a.bb = c->bb; a.prb = c->prb; a.rho_ext = c->rho_ext;
+  a.asc = c->asc; a.part = c->apart;
+  a.alpha = c->p.av_alpha; a.beta = c->p.av_beta; a.gamma = c->p.gamma; a.cn1 = c->p.cn1; a.cn2 = c->p.cn2;
+  a.eos_mode = c->p.eos_mode; a.use_psi = use_psi(c->p);
+  PhaseScope ps(c, SPH_PH_ADJOINT);
+  c->launches += launch_adjoint(a, c->gsrc, c->p.eps, c->p.G, c->p.precision, c->st);
+  // the density injection is per step
+  SPH_CUDA_TRY(cudaMemsetAsync(c->rho_ext, 0, sizeof(double) * c->n, c->st));
+  SPH_CUDA_TRY(cudaGetLastError());
+  c->kept = false;
+  return SPH_OK;
+}
 
 // internal accessors used by the reference-ABI layer (legacy.cu)
 namespace sph {

@@ -57,6 +57,35 @@ struct HydroArgs {
   int jside;  // 1: add the j-side pair force with atomics; 0: leave it to the caller
 };
 
+// arguments of the adjoint kernels (adjoint.cu)
+struct AdjArgs {
+  int n, nleaf, cap;
+  // forward state of the step (slot order)
+  const double4 *pos;     // x1, w
+  const double4 *vel;     // (v1), m
+  const double4 *hyd;     // rho, P, (u1), mu
+  const double4 *dd;      // div, curl, omega, psi
+  const double4 *dots;    // a1, du1
+  const double *vsig;
+  const double4 *old;     // v0, u0
+  const double4 *pre_acc; // a0, du0
+  const double4 *x0;      // x0 (pre-predict positions)
+  double4 *vpup;          // vp, up (recomputed)
+  const int *n_ngb, *list;
+  const double *sc;       // forward scalars: [0] dt0  [1] dt1
+  // adjoints
+  double4 *xb;  // xbar (xyz), wbar (w)
+  double4 *vb;  // vbar (xyz), ubar (w)
+  double4 *ab;  // abar (xyz), dubar (w)
+  double4 *vpb; // vpbar (xyz), upbar (w)
+  double *rhob, *Pb, *omb, *psib, *divb, *curlb, *cb, *bb, *prb;
+  const double *rho_ext;
+  double *asc;  // [0] dtbar1 in  [1] dtbar0 out  [2] vsigbar  [3] istar  [4] fbar
+  double *part;
+  double alpha, beta, gamma, cn1, cn2;
+  int eos_mode, use_psi;
+};
+
 struct StepScalars {
   // [0] dt_old  [1] dt_new  [2] time  [3..] statistics (SPH_NSTATS)
   double v[4 + SPH_NSTATS];

@@ -426,12 +426,17 @@ int launch_gravity(int n, const double4 *src, const double *h2src, double4 *out,
     else
       k_grav_f64<SPH_SOFT_SPLINE, R><<<blocks, kGThreads, 0, st>>>(n, src, h2src, out, eps2, G);
   } else {
-    constexpr int R = 4;
-    const int blocks = (n + kGThreads * R - 1) / (kGThreads * R);
-    if (soft_mode == SPH_SOFT_PLUMMER)
-      k_grav_f32x2_plummer<R / 2><<<blocks, kGThreads, 0, st>>>(n, src, out, (float)eps2, G);
-    else
+    if (soft_mode == SPH_SOFT_PLUMMER) {
+      // one i-pair per thread measured fastest at N = 1M (68 registers, more
+      // resident warps to cover the MUFU latency)
+      constexpr int RP = 1;
+      const int blocks = (n + kGThreads * 2 * RP - 1) / (kGThreads * 2 * RP);
+      k_grav_f32x2_plummer<RP><<<blocks, kGThreads, 0, st>>>(n, src, out, (float)eps2, G);
+    } else {
+      constexpr int R = 4;
+      const int blocks = (n + kGThreads * R - 1) / (kGThreads * R);
       k_grav_f32<SPH_SOFT_SPLINE, R><<<blocks, kGThreads, 0, st>>>(n, src, h2src, out, (float)eps2, G);
+    }
   }
   return 1;
 }

@@ -198,6 +198,36 @@ class Simulation:
         check(lib().cudasph_device_status(self._h, C.byref(f)), "device_status")
         return f.value
 
+    def set_time(self, time: float, dt: float):
+        check(lib().cudasph_set_time(self._h, float(time), float(dt)), "set_time")
+
+    # -- discrete adjoint ---------------------------------------------------
+    def set_keep(self, on: bool = True):
+        """Make every step keep what its reverse sweep (adjoint) needs."""
+        check(lib().cudasph_set_keep(self._h, int(on)), "set_keep")
+
+    def adjoint_set(self, name: str, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        check(lib().cudasph_adjoint_set_field(self._h, _capi.ADJ_ID[name], a.ctypes.data, 0), f"adjoint_set({name})")
+
+    def adjoint_get(self, name: str) -> np.ndarray:
+        out = np.empty(self.n, np.float64)
+        check(lib().cudasph_adjoint_get_field(self._h, _capi.ADJ_ID[name], out.ctypes.data, 0),
+              f"adjoint_get({name})")
+        return out
+
+    def adjoint_set_dt(self, dtbar: float):
+        check(lib().cudasph_adjoint_set_dt(self._h, float(dtbar)), "adjoint_set_dt")
+
+    def adjoint_get_dt(self) -> float:
+        d = C.c_double()
+        check(lib().cudasph_adjoint_get_dt(self._h, C.byref(d)), "adjoint_get_dt")
+        return d.value
+
+    def adjoint(self):
+        """Reverse sweep of the last step (taken with set_keep(True))."""
+        self._call("adjoint")
+
     # -- instrumentation ---------------------------------------------------
     def set_profiling(self, on: bool):
         check(lib().cudasph_set_profiling(self._h, int(on)), "set_profiling")

@@ -168,13 +168,37 @@ int cudasph_get_solve_evals(sph_ctx *ctx, int *dst);
 /* instrumentation: CUDA-event time of each phase, summed since the last reset */
 enum {
   SPH_PH_SORT = 0, SPH_PH_PREDICT, SPH_PH_TREE, SPH_PH_SOLVE, SPH_PH_FIND, SPH_PH_DENSITY,
-  SPH_PH_PRESSURE, SPH_PH_HYDRO, SPH_PH_GRAVITY, SPH_PH_FINISH, SPH_PH_KICK, SPH_NPHASES
+  SPH_PH_PRESSURE, SPH_PH_HYDRO, SPH_PH_GRAVITY, SPH_PH_FINISH, SPH_PH_KICK, SPH_PH_ADJOINT, SPH_NPHASES
 };
 int cudasph_set_profiling(sph_ctx *ctx, int on);
 int cudasph_phase_times(sph_ctx *ctx, double *ms /* SPH_NPHASES */, int *launches /* SPH_NPHASES */);
 int cudasph_reset_counters(sph_ctx *ctx);
 /* kernels launched by this context since the last reset */
 long long cudasph_kernel_launches(const sph_ctx *ctx);
+
+/* ---------------------------------------------------------------------- */
+/* discrete adjoint of one step (no counterpart in the reference; the      */
+/* differentiation form of the step).  With keep on, each step saves what  */
+/* its reverse sweep needs; cudasph_adjoint then maps the adjoints of the  */
+/* post-step state (x, v, u, a, du, dt) plus an optional adjoint of the    */
+/* step's density (SPH_ADJ_RHO, consumed by the call) to the adjoints of   */
+/* the pre-step state, in place.  The h solve is differentiated through    */
+/* its implicit derivative; the forward neighbour lists are reused.        */
+/* Plummer softening only.                                                 */
+/* ---------------------------------------------------------------------- */
+enum {
+  SPH_ADJ_X = 0, SPH_ADJ_Y, SPH_ADJ_Z,
+  SPH_ADJ_VX, SPH_ADJ_VY, SPH_ADJ_VZ, SPH_ADJ_U,
+  SPH_ADJ_AX, SPH_ADJ_AY, SPH_ADJ_AZ, SPH_ADJ_DU,
+  SPH_ADJ_RHO,
+  SPH_NADJ
+};
+int cudasph_set_keep(sph_ctx *ctx, int on);
+int cudasph_adjoint_set_field(sph_ctx *ctx, int field, const double *src, int on_device);
+int cudasph_adjoint_get_field(sph_ctx *ctx, int field, double *dst, int on_device);
+int cudasph_adjoint_set_dt(sph_ctx *ctx, double dtbar);
+int cudasph_adjoint_get_dt(sph_ctx *ctx, double *dtbar);
+int cudasph_adjoint(sph_ctx *ctx);
 
 /* ---------------------------------------------------------------------- */
 /* stand-alone operators on caller-owned device buffers                    */
