@@ -45,6 +45,24 @@ def test_reference_boundary_is_exported():
     assert set(REFERENCE_SYMBOLS) <= set(_capi.declared_symbols(HEADERS))
 
 
+def test_reference_driver_objects_resolve_against_this_library():
+    """Every symbol of the reference's boundary that the reference driver's
+    objects import is exported here (the objects are built from the reference
+    sources by `make -C oracle driver`, where the reference tree exists)."""
+    ref_dir = os.path.join(ROOT, "oracle", "_ref")
+    objs = [os.path.join(ref_dir, f) for f in sorted(os.listdir(ref_dir))] if os.path.isdir(ref_dir) else []
+    objs = [o for o in objs if os.path.basename(o).startswith("drv_") and o.endswith(".o")]
+    if not objs:
+        pytest.skip("reference driver objects not built")
+    und = set()
+    for o in objs:
+        out = subprocess.run(["nm", "-u", o], capture_output=True, text=True, check=True).stdout
+        und |= {ln.split()[-1] for ln in out.splitlines() if ln.strip()}
+    wanted = und & set(REFERENCE_SYMBOLS)
+    assert {"host_solve_range", "host_sph_accelerations", "compute_CUDA_gravity"} <= wanted
+    assert wanted <= _exports()
+
+
 def test_default_params_are_the_reference_constants():
     p = _capi.lib().cudasph_default_params()
     assert p.n_target == 24.0        # DESIRED_NGB, dev_solve_range.cu:14
