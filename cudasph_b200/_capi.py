@@ -92,6 +92,7 @@ def lib():
     L.cudasph_fma_peak.argtypes = [ip, ip, vp]
     L.cudasph_fma_peak.restype = C.c_double
     L.cudasph_set_keep.argtypes = [vp, ip]
+    L.cudasph_set_graph.argtypes = [vp, ip]
     L.cudasph_adjoint_set_field.argtypes = [vp, ip, vp, ip]
     L.cudasph_adjoint_get_field.argtypes = [vp, ip, vp, ip]
     L.cudasph_adjoint_set_dt.argtypes = [vp, dp]

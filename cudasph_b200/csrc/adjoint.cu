@@ -426,7 +426,19 @@ __global__ void __launch_bounds__(128) k_adj_hydro(AdjArgs a) {
 
 // -- 7. signal-speed adjoint at the arg-min particle of the timestep ---------
 // vsig_i = max_j vs_ij, vs = c_i + c_j - beta drdv / ds (drdv < 0) else c_i + c_j;
-// the adjoint goes to the first pair (list order) that attains the maximum.
+// the adjoint goes to the first pair (list order) that attains the maximum,
+// recomputed here in FP64 (the mixed form's forward value is FP32).
+__device__ __forceinline__ double pair_vs(const AdjArgs &a, int s, int j, double c_i, double4 pi, double4 vi) {
+  const double4 pj = a.pos[j], vj = a.vpup[j], hj = a.hyd[j];
+  const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+  const double dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
+  const double ds = sqrt(dx * dx + dy * dy + dz * dz);
+  const double drdv = dx * dvx + dy * dvy + dz * dvz;
+  double vs = c_i + sqrt(a.gamma * hj.y / hj.x);
+  if (drdv < 0) vs -= a.beta * drdv / ds;
+  return vs;
+}
+
 __global__ void k_adj_vsig(AdjArgs a) {
   if (threadIdx.x != 0) return;
   const double vsb = a.asc[2];
@@ -437,18 +449,21 @@ __global__ void k_adj_vsig(AdjArgs a) {
   const double4 pi = a.pos[s], vi = a.vpup[s], hi4 = a.hyd[s];
   const double gam = a.gamma, beta = a.beta;
   const double c_i = sqrt(gam * hi4.y / hi4.x);
-  const double target = a.vsig[s];
+  int kbest = -1;
+  double best = -1e300;
   for (int k = 0; k < cnt; k++) {
     const int j = a.list[((size_t)leaf * a.cap + k) * kLeaf + lane];
-    const double4 pj = a.pos[j], vj = a.vpup[j], hj = a.hyd[j];
+    const double vs = pair_vs(a, s, j, c_i, pi, vi);
+    if (vs > best) { best = vs; kbest = k; }
+  }
+  if (kbest < 0) return;
+  {
+    const int j = a.list[((size_t)leaf * a.cap + kbest) * kLeaf + lane];
+    const double4 pj = a.pos[j], vj = a.vpup[j];
     const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
     const double dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
     const double ds = sqrt(dx * dx + dy * dy + dz * dz);
     const double drdv = dx * dvx + dy * dvy + dz * dvz;
-    const double c_j = sqrt(gam * hj.y / hj.x);
-    double vs = c_i + c_j;
-    if (drdv < 0) vs -= beta * drdv / ds;
-    if (fabs(vs - target) > 1e-12 * fabs(target)) continue;
     a.cb[s] += vsb;
     a.cb[j] += vsb;
     if (drdv < 0 && ds > 0) {
@@ -460,7 +475,6 @@ __global__ void k_adj_vsig(AdjArgs a) {
       a.vpb[s].x += drdvb * dx; a.vpb[s].y += drdvb * dy; a.vpb[s].z += drdvb * dz;
       a.vpb[j].x -= drdvb * dx; a.vpb[j].y -= drdvb * dy; a.vpb[j].z -= drdvb * dz;
     }
-    return;
   }
 }
 

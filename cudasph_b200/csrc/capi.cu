@@ -93,12 +93,19 @@ struct sph_ctx {
   bool profiling = false;
   std::vector<cudaEvent_t> ev[SPH_NPHASES];
   std::vector<cudaEvent_t> pool;
+  // CUDA graphs of one whole step, one per parity of the double-buffered
+  // state (the sort flips the buffers every step)
+  bool use_graph = false;
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  long long glaunches[2] = {0, 0};
   // adjoint (allocated on the first cudasph_set_keep(ctx, 1))
   bool keep = false, kept = false;
   double4 *pre_acc = nullptr, *xb = nullptr, *vb = nullptr, *ab = nullptr, *vpb = nullptr, *vpup = nullptr;
   double *rhob = nullptr, *Pb = nullptr, *omb = nullptr, *psib = nullptr, *divb = nullptr, *curlb = nullptr;
   double *cb = nullptr, *bb = nullptr, *prb = nullptr, *rho_ext = nullptr, *asc = nullptr, *apart = nullptr;
 };
+
+static void drop_graphs(sph_ctx *c);
 
 namespace {
 
@@ -245,6 +252,7 @@ extern "C" int cudasph_destroy(sph_ctx *c) {
   for (int ph = 0; ph < SPH_NPHASES; ph++)
     for (cudaEvent_t e : c->ev[ph]) cudaEventDestroy(e);
   for (cudaEvent_t e : c->pool) cudaEventDestroy(e);
+  drop_graphs(c);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
   return SPH_OK;
@@ -335,6 +343,8 @@ extern "C" int cudasph_set_params(sph_ctx *c, const sph_params *p) {
   int rc = check_params(p);
   if (rc) return rc;
   SPH_CUDA_TRY(cudaSetDevice(c->device));
+  SPH_CUDA_TRY(cudaStreamSynchronize(c->st));
+  drop_graphs(c);  // parameters are baked into captured launches
   c->p = *p;
   return alloc_lists(c);
 }
@@ -640,8 +650,67 @@ extern "C" int cudasph_kick(sph_ctx *c) {
   return SPH_OK;
 }
 
+static void drop_graphs(sph_ctx *c) {
+  for (int k = 0; k < 2; k++) {
+    if (c->gexec[k]) cudaGraphExecDestroy(c->gexec[k]);
+    c->gexec[k] = nullptr;
+    c->glaunches[k] = 0;
+  }
+}
+
+static int step_body(sph_ctx *c);
+
+// One step, replayed from a captured CUDA graph when the step is the steady
+// kind (sorted every step, no profiling events, no adjoint bookkeeping): the
+// ~45 launches of a step then cost one graph launch.  The first step of each
+// buffer parity runs under stream capture; the host bookkeeping it performs
+// (buffer flip, phase validity) is then repeated by hand on every replay.
 extern "C" int cudasph_step(sph_ctx *c) {
   if (!c) return SPH_ERR_ARG;
+  const bool graphable = c->use_graph && !c->need_sort && c->p.sort_every == 1 && !c->profiling && !c->keep;
+  if (!graphable) return step_body(c);
+  SPH_CUDA_TRY(cudaSetDevice(c->device));
+  const int par = c->cur;
+  if (c->gexec[par]) {
+    SPH_CUDA_TRY(cudaGraphLaunch(c->gexec[par], c->st));
+    c->iteration++;
+    c->cur = 1 - c->cur;
+    c->tree_ok = c->lists_ok = c->density_ok = true;
+    c->kept = false;
+    c->launches += c->glaunches[par];
+    return SPH_OK;
+  }
+  const long long l0 = c->launches;
+  SPH_CUDA_TRY(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+  int rc = step_body(c);
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(c->st, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return sph_internal_cuda_fail(e, "cudaStreamEndCapture", __FILE__, __LINE__);
+  e = cudaGraphInstantiate(&c->gexec[par], g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    c->gexec[par] = nullptr;
+    return sph_internal_cuda_fail(e, "cudaGraphInstantiate", __FILE__, __LINE__);
+  }
+  c->glaunches[par] = c->launches - l0;
+  SPH_CUDA_TRY(cudaGraphLaunch(c->gexec[par], c->st));
+  return SPH_OK;
+}
+
+extern "C" int cudasph_set_graph(sph_ctx *c, int on) {
+  if (!c) return SPH_ERR_ARG;
+  SPH_CUDA_TRY(cudaSetDevice(c->device));
+  SPH_CUDA_TRY(cudaStreamSynchronize(c->st));
+  if (!on) drop_graphs(c);
+  c->use_graph = on != 0;
+  return SPH_OK;
+}
+
+static int step_body(sph_ctx *c) {
   int rc;
   c->iteration++;
   if (c->need_sort || (c->p.sort_every > 0 && c->iteration % c->p.sort_every == 0))

@@ -25,7 +25,53 @@ constexpr unsigned kFull = 0xffffffffu;
 struct WarpSmem {
   int stack[kStack];
   double sx[kLeaf], sy[kLeaf], sz[kLeaf];
+  float4 sf[kLeaf];  // anchor-relative FP32 copies for the pre-filter
 };
+
+// Conservative FP32 pre-filter of the neighbour predicate.  Coordinates are
+// taken relative to a warp anchor (lane 0's particle) and rounded to FP32.
+// For a pair that is truly within range w of lane l, |x_j - anchor| <= B + w
+// where B bounds |x_l - anchor| over the warp, so the FP32 squared distance
+// differs from the exact one by less than w^2 (4.2e-7 (B + w)/w + 2.6e-7).
+// A candidate is rejected only when its FP32 squared distance exceeds
+// w^2 (1 + m) with m = 1e-6 (B + w)/w + 1e-6, i.e. when it is certainly
+// outside; everything else goes through the exact FP64 predicate, so the
+// neighbour sets are unchanged.  Lanes with m > 1e-2 skip the pre-filter.
+struct Prefilter {
+  double ax, ay, az;  // warp anchor
+  double B;           // sqrt(3) max |x_l - anchor| over the warp
+  float xf, yf, zf;   // this lane, anchor-relative
+};
+
+__device__ __forceinline__ Prefilter make_prefilter(bool on, double x, double y, double z) {
+  Prefilter f;
+  f.ax = __shfl_sync(0xffffffffu, x, 0);
+  f.ay = __shfl_sync(0xffffffffu, y, 0);
+  f.az = __shfl_sync(0xffffffffu, z, 0);
+  const double dx = x - f.ax, dy = y - f.ay, dz = z - f.az;
+  double b = on ? fmax(fabs(dx), fmax(fabs(dy), fabs(dz))) : 0.0;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
+  f.B = 1.7320508075688772 * b;
+  f.xf = (float)dx;
+  f.yf = (float)dy;
+  f.zf = (float)dz;
+  return f;
+}
+
+// the FP32 threshold for range w; negative = no pre-filter for this lane
+__device__ __forceinline__ float prefilter_threshold(const Prefilter &f, double w) {
+  if (!(w > 0)) return -1.f;
+  const double m = 1e-6 * (f.B + w) / w + 1e-6;
+  if (m > 1e-2) return -1.f;
+  return (float)(w * w * (1.0 + m));
+}
+
+__device__ __forceinline__ bool certainly_outside(const Prefilter &f, float thr, float4 q) {
+  const float dx = f.xf - q.x, dy = f.yf - q.y, dz = f.zf - q.z;
+  const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+  return thr >= 0.f && d2 > thr;
+}
 
 // Query box over the lanes that take part: [x - r, x + r] widened by a
 // relative 1e-15 of the magnitudes (covers the rounding of x - r) and
@@ -91,7 +137,8 @@ __device__ bool walk_leaves(const TreeView &t, const float *ql, const float *qh,
   return true;
 }
 
-__device__ __forceinline__ void stage_leaf(const double4 *__restrict__ pos, int n, int leaf, WarpSmem &sm) {
+__device__ __forceinline__ void stage_leaf(const double4 *__restrict__ pos, int n, int leaf, WarpSmem &sm,
+                                           const Prefilter &f) {
   const int s = leaf * kLeaf + (int)lane_id();
   __syncwarp();
   if (s < n) {
@@ -99,6 +146,7 @@ __device__ __forceinline__ void stage_leaf(const double4 *__restrict__ pos, int 
     sm.sx[lane_id()] = p.x;
     sm.sy[lane_id()] = p.y;
     sm.sz[lane_id()] = p.z;
+    sm.sf[lane_id()] = make_float4((float)(p.x - f.ax), (float)(p.y - f.ay), (float)(p.z - f.az), 0.f);
   }
   __syncwarp();
 }
@@ -132,6 +180,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_solve_range(SolveArgs a
     const double4 p = a.pos[s];
     xi = p.x; yi = p.y; zi = p.z; w = p.w;
   }
+  const Prefilter pf = make_prefilter(valid && w > 0, xi, yi, zi);
   int phase = (valid && w > 0) ? kBr0 : kDone;
   double dx = 0, f = 0, x_left = 0, f_try = 0, rx = 0, ry = 0;
   int iter = 0, keep = 0, nev = 0;
@@ -144,11 +193,13 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_solve_range(SolveArgs a
     warp_query_box(need, xi, yi, zi, w, ql, qh);
     double sf = 0, sg = 0, sc = 0;
     const double w2 = __dmul_rn(w, w);
+    const float thr = prefilter_threshold(pf, w);
     stack_ok &= walk_leaves(a.t, ql, qh, sm.stack, [&](int lj) {
-      stage_leaf(a.pos, n, lj, sm);
+      stage_leaf(a.pos, n, lj, sm, pf);
       const int cnt = min(kLeaf, n - lj * kLeaf);
       if (need) {
         for (int k = 0; k < cnt; k++) {
+          if (certainly_outside(pf, thr, sm.sf[k])) continue;
           const double d2 = ds2_exact(xi - sm.sx[k], yi - sm.sy[k], zi - sm.sz[k]);
           if (d2 < w2) {
             const double u = 2 * sqrt(d2) / w;
@@ -262,16 +313,19 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_find_ngb(FindArgs a) {
   float ql[3], qh[3];
   warp_query_box(on, xi, yi, zi, w, ql, qh);
   const double w2 = __dmul_rn(w, w);
+  const Prefilter pf = make_prefilter(on, xi, yi, zi);
+  const float thr = prefilter_threshold(pf, w);
   int cnt = 0;
   int *out = a.list + (size_t)leaf * a.cap * kLeaf + lane_id();
   const int cap = a.cap;
   bool ok = true;
   if (__any_sync(kFull, on)) {
     ok = walk_leaves(a.t, ql, qh, sm.stack, [&](int lj) {
-      stage_leaf(a.pos, n, lj, sm);
+      stage_leaf(a.pos, n, lj, sm, pf);
       const int m = min(kLeaf, n - lj * kLeaf);
       if (on) {
         for (int k = 0; k < m; k++) {
+          if (certainly_outside(pf, thr, sm.sf[k])) continue;
           const double d2 = ds2_exact(xi - sm.sx[k], yi - sm.sy[k], zi - sm.sz[k]);
           if (d2 < w2) {
             if (cnt < cap) out[(size_t)cnt * kLeaf] = lj * kLeaf + k;

@@ -198,6 +198,10 @@ class Simulation:
         check(lib().cudasph_device_status(self._h, C.byref(f)), "device_status")
         return f.value
 
+    def set_graph(self, on: bool = True):
+        """Replay steady steps from a captured CUDA graph."""
+        check(lib().cudasph_set_graph(self._h, int(on)), "set_graph")
+
     def set_time(self, time: float, dt: float):
         check(lib().cudasph_set_time(self._h, float(time), float(dt)), "set_time")
 

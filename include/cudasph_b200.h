@@ -151,6 +151,10 @@ int cudasph_gravity(sph_ctx *ctx);           /* sph_grav_kernel.cu:179 */
 int cudasph_finish(sph_ctx *ctx);            /* a += g, diagnostics, timestep (step.cpp:96-127) */
 int cudasph_kick(sph_ctx *ctx);              /* step.cpp:128-134 */
 int cudasph_step(sph_ctx *ctx);              /* the whole step */
+/* Replay steady steps (sorted every step, profiling and keep off) from a
+ * captured CUDA graph: one graph launch per step instead of ~45 launches.
+ * Changing parameters drops the captured graphs. */
+int cudasph_set_graph(sph_ctx *ctx, int on);
 int cudasph_steps(sph_ctx *ctx, int k);      /* k whole steps */
 
 /* End-to-end step through host buffers, the way the reference driver owns
