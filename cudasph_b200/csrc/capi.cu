@@ -20,7 +20,7 @@ int morton_keys(int n, const double4 *pos, const double *x, const double *y, con
 int tree_layout(int n, TreeView *t);
 int build_tree(const TreeView &t, const double4 *pos, float4 *lo, float4 *hi, cudaStream_t st);
 int launch_solve_range(const TreeView &t, double4 *pos, int *nevals, unsigned *flags, const sph_params &p,
-                       cudaStream_t st);
+                       int *n_ngb, int *list, int cap, cudaStream_t st);
 int launch_find_ngb(const TreeView &t, const double4 *pos, int *n_ngb, int *list, int cap, unsigned *flags,
                     cudaStream_t st);
 int launch_density(const HydroArgs &a, cudaStream_t st);
@@ -551,8 +551,11 @@ extern "C" int cudasph_solve_range(sph_ctx *c) {
   }
   SPH_CUDA_TRY(cudaSetDevice(c->device));
   PhaseScope ps(c, SPH_PH_SOLVE);
-  LAUNCHED(launch_solve_range(c->tree, c->f[c->cur].pos, c->nevals, c->flags, c->p, c->st));
-  c->lists_ok = c->density_ok = false;
+  LAUNCHED(launch_solve_range(c->tree, c->f[c->cur].pos, c->nevals, c->flags, c->p, c->n_ngb, c->list, c->list_cap,
+                              c->st));
+  // the solve writes the neighbour lists at the final ranges (find_ngb fused)
+  c->lists_ok = true;
+  c->density_ok = false;
   SPH_CUDA_TRY(cudaGetLastError());
   return SPH_OK;
 }
@@ -563,6 +566,7 @@ extern "C" int cudasph_find_ngb(sph_ctx *c) {
     int rc = cudasph_build_tree(c);
     if (rc) return rc;
   }
+  if (c->lists_ok) return SPH_OK;  // already written by the h solve at these ranges
   SPH_CUDA_TRY(cudaSetDevice(c->device));
   PhaseScope ps(c, SPH_PH_FIND);
   LAUNCHED(launch_find_ngb(c->tree, c->f[c->cur].pos, c->n_ngb, c->list, c->list_cap, c->flags, c->st));

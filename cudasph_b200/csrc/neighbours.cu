@@ -158,6 +158,9 @@ struct SolveArgs {
   unsigned *flags;
   double n_target, rel_err, f_scale;
   int max_iter;
+  int *n_ngb;  // hard count at the final range
+  int *list;   // neighbour lists at the final range (layout of k_find_ngb)
+  int cap;
 };
 
 enum { kBr0 = 0, kBr1 = 1, kSolve = 2, kDone = 3 };
@@ -186,31 +189,52 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_solve_range(SolveArgs a
   int iter = 0, keep = 0, nev = 0;
   bool stack_ok = true;
   const double rel = a.rel_err, fs = a.f_scale;
+  // Every evaluation also writes the lane's neighbour list at the range it
+  // evaluates (find_ngb fused in): the final range is the last one evaluated,
+  // except when the bracket converges at once and the midpoint of
+  // (w - |dx|/2, w + |dx|/2) rounds away from w -- then one list-only round
+  // at the final range follows (`pending`).
+  int *out = a.list + (size_t)leaf * a.cap * kLeaf + lane_id();
+  const int cap = a.cap;
+  double w_list = -1.0;
+  int cnt_list = 0;
+  bool pending = false;
   while (true) {
-    const bool need = phase != kDone;
+    const bool iterate = phase != kDone;
+    const bool need = iterate || pending;
     if (!__any_sync(kFull, need)) break;
     float ql[3], qh[3];
     warp_query_box(need, xi, yi, zi, w, ql, qh);
-    double sf = 0, sg = 0, sc = 0;
+    double sf = 0, sg = 0;
+    int c = 0;
     const double w2 = __dmul_rn(w, w);
     const float thr = prefilter_threshold(pf, w);
     stack_ok &= walk_leaves(a.t, ql, qh, sm.stack, [&](int lj) {
       stage_leaf(a.pos, n, lj, sm, pf);
-      const int cnt = min(kLeaf, n - lj * kLeaf);
+      const int cntj = min(kLeaf, n - lj * kLeaf);
       if (need) {
-        for (int k = 0; k < cnt; k++) {
+        for (int k = 0; k < cntj; k++) {
           if (certainly_outside(pf, thr, sm.sf[k])) continue;
           const double d2 = ds2_exact(xi - sm.sx[k], yi - sm.sy[k], zi - sm.sz[k]);
           if (d2 < w2) {
-            const double u = 2 * sqrt(d2) / w;
-            sf += k_ig<double>(u);
-            sg -= k_digdh<double>(u);
-            sc += 1;
+            if (c < cap) out[(size_t)c * kLeaf] = lj * kLeaf + k;
+            c++;
+            if (iterate) {
+              const double u = 2 * sqrt(d2) / w;
+              sf += k_ig<double>(u);
+              sg -= k_digdh<double>(u);
+            }
           }
         }
       }
     });
     if (!need) continue;
+    w_list = w;
+    cnt_list = c;
+    if (!iterate) {
+      pending = false;
+      continue;
+    }
     nev++;
     // compute_ngb epilogue, dev_solve_range.cu:77-87
     f = sf - a.n_target;
@@ -275,10 +299,13 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_solve_range(SolveArgs a
         phase = kDone;
       }
     }
+    pending = (phase == kDone) && (w != w_list);
   }
   if (!stack_ok && lane_id() == 0) raise_flag(a.flags, SPH_FLAG_STACK_OVERFLOW);
+  if (cnt_list > cap) raise_flag(a.flags, SPH_FLAG_NGB_OVERFLOW);
   if (valid) {
     a.pos[s].w = (w > 0) ? w : 0.0;
+    a.n_ngb[s] = cnt_list;
     if (a.nevals) a.nevals[s] = nev;
   }
 }
@@ -341,9 +368,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_find_ngb(FindArgs a) {
 }
 
 int launch_solve_range(const TreeView &t, double4 *pos, int *nevals, unsigned *flags, const sph_params &p,
-                       cudaStream_t st) {
+                       int *n_ngb, int *list, int cap, cudaStream_t st) {
   SolveArgs a;
   a.t = t; a.pos = pos; a.nevals = nevals; a.flags = flags;
+  a.n_ngb = n_ngb; a.list = list; a.cap = cap;
   a.n_target = p.n_target; a.rel_err = p.rel_err; a.f_scale = p.f_scale; a.max_iter = p.max_iter;
   const int warps = t.count[0];
   k_solve_range<<<(warps + kWarpsPerBlock - 1) / kWarpsPerBlock, kWarpsPerBlock * 32, 0, st>>>(a);
