@@ -328,12 +328,18 @@ __device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
   return d;
 }
 
+// One-sided form: every i of the block against the sources [jlo, jhi); with
+// tile > 0 the range is the tile of `tile` particles that holds the block
+// (the diagonal tiles of the symmetric form), else all n.
 template <int RP>  // i-particle pairs per thread
 __global__ void __launch_bounds__(kGThreads) k_grav_f32x2_plummer(int n, const double4 *__restrict__ src,
-                                                                  double4 *__restrict__ out, float eps2, double G) {
+                                                                  double4 *__restrict__ out, float eps2, double G,
+                                                                  int tile) {
   __shared__ ulonglong2 sj[kGThreads][2];
   const int t = threadIdx.x;
   const int i0 = blockIdx.x * kGThreads * 2 * RP;
+  const int jlo = tile > 0 ? (i0 / tile) * tile : 0;
+  const int jhi = tile > 0 ? min(jlo + tile, n) : n;
   const double4 anc = src[min(i0, n - 1)];
   f32x2 xi[RP], yi[RP], zi[RP];
   float ahi[2 * RP][4], alo[2 * RP][4];
@@ -350,10 +356,10 @@ __global__ void __launch_bounds__(kGThreads) k_grav_f32x2_plummer(int n, const d
 #pragma unroll
     for (int c = 0; c < 4; c++) ahi[r][c] = alo[r][c] = 0.f;
   const f32x2 e2 = pk2(eps2, eps2);
-  for (int j0 = 0; j0 < n; j0 += kGThreads) {
+  for (int j0 = jlo; j0 < jhi; j0 += kGThreads) {
     const int j = j0 + t;
     __syncthreads();
-    if (j < n) {
+    if (j < jhi) {
       const double4 q = src[j];
       const float x = (float)(q.x - anc.x), y = (float)(q.y - anc.y), z = (float)(q.z - anc.z), m = (float)q.w;
       sj[t][0] = make_ulonglong2(pk2(x, x), pk2(y, y));
@@ -413,6 +419,167 @@ __global__ void __launch_bounds__(kGThreads) k_grav_f32x2_plummer(int n, const d
   }
 }
 
+// ------------------ mixed (FP32), symmetric pair form -----------------------
+// Plummer gravity computing each pair once (Newton's third law): the force
+// of a pair is applied to i and, with the opposite sign and i's mass, to j.
+// Per two pairs (one packed i-pair against one j) the loop issues 19 packed
+// FP32 instructions and 2 MUFU.rsq, against 26 and 4 when both directions
+// are computed separately.
+//
+// Work split: the Morton order is cut into tiles of kSymTile particles; a
+// block owns one i-tile (kSymWarps warps, kSymRP packed i-pairs per lane) and
+// one work item = up to kSymChunk j-tiles strictly above its own, so the
+// upper triangle of tile pairs is covered once; the diagonal tiles run
+// through the one-sided kernel.  Inside a warp the j's travel: a batch of 32
+// sources, one per lane, rotates through the lanes by shuffles, each lane
+// meeting every source of the batch once; a source carries its own
+// accumulator with it, so after 32 steps lane l holds the batch-partial of
+// source l.  The partials of the block's warps are summed in shared memory
+// (FP64) and added to the output with FP64 atomics; the i-side partials fold
+// after every batch into FP64 accumulators kept in shared memory (registers
+// go to the eight i-pairs a lane carries: many independent pairs per lane
+// hide the MUFU and shuffle latencies better than more resident warps, as a
+// sweep of warps x i-pairs per lane at N = 1M showed: 2 x 8 took 357 ms,
+// 4 x 5 360 ms, 4 x 4 371 ms, 8 x 2 with FP64 registers 412 ms) and are
+// added to the output at the end of the item.
+// The output therefore holds the diagonal-tile sums first (stored by the
+// one-sided kernel) and receives the off-diagonal sums by atomics, so the
+// order of the FP64 additions, not their values, varies between runs.
+constexpr int kSymWarps = 2;
+constexpr int kSymRP = 8;
+constexpr int kSymTile = kSymWarps * 64 * kSymRP;  // 1024 i-particles per block
+constexpr int kSymChunk = 8;                        // j-tiles per work item
+
+// S(M) = sum_{m=1..M} ceil(m / kSymChunk): items of the rows with 1..M tiles
+__host__ __device__ __forceinline__ long long sym_S(long long M) {
+  const long long q = M / kSymChunk, r = M % kSymChunk;
+  return kSymChunk * q * (q + 1) / 2 + (q + 1) * r;
+}
+// first work item of tile row b (row b has nt - 1 - b tiles above the diagonal)
+__host__ __device__ __forceinline__ long long sym_first(int b, int nt) { return sym_S(nt - 1) - sym_S(nt - 1 - b); }
+
+__global__ void __launch_bounds__(kSymWarps * 32, 4) k_grav_sym_plummer(int n, int nt, const double4 *__restrict__ src,
+                                                                         double4 *__restrict__ out, float eps2,
+                                                                         double G) {
+  __shared__ float red[2][kSymWarps][4][32];
+  __shared__ double iacc[2 * kSymRP * 4][kSymWarps * 32];  // [i-slot * 4 + component][thread]
+  const long long item = blockIdx.x;
+  int lo = 0, hi = nt - 2;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (sym_first(mid, nt) <= item) lo = mid; else hi = mid - 1;
+  }
+  const int b = lo;
+  const int t_lo = b + 1 + (int)(item - sym_first(b, nt)) * kSymChunk;
+  const int t_hi = min(t_lo + kSymChunk, nt);
+  const int j_lo = t_lo * kSymTile, j_hi = min(t_hi * kSymTile, n);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nxt = (l + 1) & 31;
+  const int i0 = b * kSymTile;
+  const double4 anc = src[i0];
+  const int ib = i0 + w * 64 * kSymRP + l;
+
+  f32x2 xi[kSymRP], yi[kSymRP], zi[kSymRP], nmi[kSymRP];
+#pragma unroll
+  for (int p = 0; p < kSymRP; p++) {
+    float x[2] = {0.f, 0.f}, y[2] = {0.f, 0.f}, z[2] = {0.f, 0.f}, m[2] = {0.f, 0.f};
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int i = ib + (2 * p + h) * 32;
+      if (i < n) {
+        const double4 q = src[i];
+        x[h] = (float)(q.x - anc.x); y[h] = (float)(q.y - anc.y); z[h] = (float)(q.z - anc.z); m[h] = -(float)q.w;
+      }
+#pragma unroll
+      for (int c = 0; c < 4; c++) iacc[(2 * p + h) * 4 + c][threadIdx.x] = 0.0;
+    }
+    xi[p] = pk2(x[0], x[1]); yi[p] = pk2(y[0], y[1]); zi[p] = pk2(z[0], z[1]); nmi[p] = pk2(m[0], m[1]);
+  }
+  const f32x2 e2 = pk2(eps2, eps2);
+  int k = 0;
+  for (int jb = j_lo; jb < j_hi; jb += 32, k ^= 1) {
+    float xj = 0.f, yj = 0.f, zj = 0.f, mj = 0.f;  // padding source: at the anchor, massless
+    if (jb + l < j_hi) {
+      const double4 q = src[jb + l];
+      xj = (float)(q.x - anc.x); yj = (float)(q.y - anc.y); zj = (float)(q.z - anc.z); mj = (float)q.w;
+    }
+    float ajx = 0.f, ajy = 0.f, ajz = 0.f, ajp = 0.f;
+    f32x2 px[kSymRP], py[kSymRP], pz[kSymRP], pp[kSymRP];
+#pragma unroll
+    for (int p = 0; p < kSymRP; p++) px[p] = py[p] = pz[p] = pp[p] = 0ull;
+#pragma unroll 1
+    for (int s = 0; s < 32; s++) {
+      const f32x2 XJ = pk2(xj, xj), YJ = pk2(yj, yj), ZJ = pk2(zj, zj), MJ = pk2(mj, mj);
+      f32x2 AX = pk2(ajx, 0.f), AY = pk2(ajy, 0.f), AZ = pk2(ajz, 0.f), AP = pk2(ajp, 0.f);
+#pragma unroll
+      for (int p = 0; p < kSymRP; p++) {
+        const f32x2 dx = sub2(XJ, xi[p]), dy = sub2(YJ, yi[p]), dz = sub2(ZJ, zi[p]);
+        f32x2 r2 = fma2(dx, dx, e2);
+        r2 = fma2(dy, dy, r2);
+        r2 = fma2(dz, dz, r2);
+        float r2a, r2b;
+        upk2(r2, r2a, r2b);
+        const f32x2 inv = pk2(rsqrt_f32(r2a), rsqrt_f32(r2b));
+        const f32x2 inv3 = mul2(mul2(inv, inv), inv);
+        const f32x2 qx = mul2(dx, inv3), qy = mul2(dy, inv3), qz = mul2(dz, inv3);
+        px[p] = fma2(MJ, qx, px[p]);
+        py[p] = fma2(MJ, qy, py[p]);
+        pz[p] = fma2(MJ, qz, pz[p]);
+        pp[p] = fma2(MJ, inv, pp[p]);
+        AX = fma2(nmi[p], qx, AX);
+        AY = fma2(nmi[p], qy, AY);
+        AZ = fma2(nmi[p], qz, AZ);
+        AP = fma2(nmi[p], inv, AP);
+      }
+      float a0, a1;
+      upk2(AX, a0, a1); ajx = a0 + a1;
+      upk2(AY, a0, a1); ajy = a0 + a1;
+      upk2(AZ, a0, a1); ajz = a0 + a1;
+      upk2(AP, a0, a1); ajp = a0 + a1;
+      xj = __shfl_sync(0xffffffffu, xj, nxt);
+      yj = __shfl_sync(0xffffffffu, yj, nxt);
+      zj = __shfl_sync(0xffffffffu, zj, nxt);
+      mj = __shfl_sync(0xffffffffu, mj, nxt);
+      ajx = __shfl_sync(0xffffffffu, ajx, nxt);
+      ajy = __shfl_sync(0xffffffffu, ajy, nxt);
+      ajz = __shfl_sync(0xffffffffu, ajz, nxt);
+      ajp = __shfl_sync(0xffffffffu, ajp, nxt);
+    }
+#pragma unroll
+    for (int p = 0; p < kSymRP; p++) {
+      const f32x2 part[4] = {px[p], py[p], pz[p], pp[p]};
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        float a0, a1;
+        upk2(part[c], a0, a1);
+        if (c == 3) a0 = -a0, a1 = -a1;  // pp holds +m/r
+        iacc[(2 * p) * 4 + c][threadIdx.x] += a0;
+        iacc[(2 * p + 1) * 4 + c][threadIdx.x] += a1;
+      }
+    }
+    red[k][w][0][l] = ajx;
+    red[k][w][1][l] = ajy;
+    red[k][w][2][l] = ajz;
+    red[k][w][3][l] = ajp;
+    __syncthreads();  // also orders this batch's reads of red[k] before batch + 2 writes it
+    for (int q = threadIdx.x; q < 128; q += kSymWarps * 32) {
+      const int c = q >> 5, ll = q & 31;
+      double s = 0.0;
+#pragma unroll
+      for (int v = 0; v < kSymWarps; v++) s += (double)red[k][v][c][ll];
+      if (jb + ll < j_hi) atomicAdd(&reinterpret_cast<double *>(out + jb + ll)[c], G * s);
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 2 * kSymRP; r++) {
+    const int i = ib + r * 32;
+    if (i < n) {
+      double *o = reinterpret_cast<double *>(out + i);
+#pragma unroll
+      for (int c = 0; c < 4; c++) atomicAdd(o + c, G * iacc[r * 4 + c][threadIdx.x]);
+    }
+  }
+}
+
 // src = {x, y, z, m} per particle; h2src = range^2 (spline mode only)
 int launch_gravity(int n, const double4 *src, const double *h2src, double4 *out, int soft_mode, double eps, double G,
                    int precision, cudaStream_t st) {
@@ -430,8 +597,17 @@ int launch_gravity(int n, const double4 *src, const double *h2src, double4 *out,
       // one i-pair per thread measured fastest at N = 1M (68 registers, more
       // resident warps to cover the MUFU latency)
       constexpr int RP = 1;
+      static_assert(kSymTile % (kGThreads * 2 * RP) == 0, "diagonal tiles must hold whole blocks");
       const int blocks = (n + kGThreads * 2 * RP - 1) / (kGThreads * 2 * RP);
-      k_grav_f32x2_plummer<RP><<<blocks, kGThreads, 0, st>>>(n, src, out, (float)eps2, G);
+      const int nt = (n + kSymTile - 1) / kSymTile;
+      if (nt < 2) {
+        k_grav_f32x2_plummer<RP><<<blocks, kGThreads, 0, st>>>(n, src, out, (float)eps2, G, 0);
+      } else {
+        // diagonal tiles store, the symmetric items add on top
+        k_grav_f32x2_plummer<RP><<<blocks, kGThreads, 0, st>>>(n, src, out, (float)eps2, G, kSymTile);
+        const long long items = sym_S(nt - 1);
+        k_grav_sym_plummer<<<(unsigned)items, kSymWarps * 32, 0, st>>>(n, nt, src, out, (float)eps2, G);
+      }
     } else {
       constexpr int R = 4;
       const int blocks = (n + kGThreads * R - 1) / (kGThreads * R);

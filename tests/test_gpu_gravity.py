@@ -1,0 +1,82 @@
+"""Direct-N gravity through the standalone entry point cudasph_gravity_direct.
+
+The mixed Plummer form computes each pair once above the diagonal tiles of
+1,024 particles (work items of up to 8 tiles) and the diagonal tiles
+one-sided, so the sizes below cover: a single tile, an exact tile, a ragged
+second tile, rows split over several work items with a ragged last batch.
+Reference: the FP64 oracle restatement of sph_grav_kernel.cu:14-111 (Plummer
+mode) on the same particles.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [1000, 1024, 1025, 2048, 5000, 20001]
+
+
+def _cloud(n, seed, condensed=False):
+    rs = np.random.default_rng(seed)
+    # a uniform ball, or a centrally condensed cloud; both with coincident pairs
+    r = rs.random(n) ** 2 if condensed else rs.random(n) ** (1.0 / 3.0)
+    v = rs.normal(size=(n, 3))
+    p = v / np.linalg.norm(v, axis=1)[:, None] * r[:, None]
+    p[1::97] = p[0::97][: p[1::97].shape[0]]
+    m = rs.uniform(0.5, 1.5, n) / n
+    return p, m
+
+
+def _run(p, m, eps, G, precision):
+    import torch
+    from cudasph_b200._capi import lib
+    n = m.size
+    src = torch.from_numpy(np.column_stack([p, m]).astype(np.float64).copy()).cuda()
+    out = torch.full((n, 4), np.nan, dtype=torch.float64, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    rc = lib().cudasph_gravity_direct(n, src.data_ptr(), None, out.data_ptr(), 1, eps, G, precision, st)
+    assert rc == 0
+    torch.cuda.synchronize()
+    return out.cpu().numpy()
+
+
+def _oracle(p, m, eps, G):
+    par = O.make_params(soft_mode=1, eps=eps, G=G)
+    g = O.gravity(p[:, 0], p[:, 1], p[:, 2], m, np.zeros_like(m), par)
+    return np.stack(g, 1)
+
+
+# RMS force error bound of the mixed form, 1e-5: FP32 pair terms give 1e-6 to
+# 6e-6 on these clouds (their net forces cancel strongly, and close pairs lose
+# digits to FP32 rounding of the anchor-relative coordinates) on both the
+# one-sided (n <= 1024) and the symmetric path; a pair missed or counted twice
+# shows as 1e-3 or more.
+@pytest.mark.parametrize("condensed,bound", [(False, 1e-5), (True, 1e-5)])
+@pytest.mark.parametrize("n", SIZES)
+def test_mixed_plummer_gravity_matches_oracle(n, condensed, bound):
+    p, m = _cloud(n, 100 + n, condensed)
+    eps, G = 0.004, 1.3
+    got = _run(p, m, eps, G, 1)
+    ref = _oracle(p, m, eps, G)
+    assert np.all(np.isfinite(got))
+    a, r = got[:, :3], ref[:, :3]
+    rms = np.sqrt(np.mean(np.sum((a - r) ** 2, 1)) / np.mean(np.sum(r ** 2, 1)))
+    assert rms < bound, rms
+    assert np.max(np.abs(got[:, 3] / ref[:, 3] - 1)) < 1e-5
+
+
+@pytest.mark.parametrize("n", [1025, 20001])
+def test_fp64_plummer_gravity_matches_oracle(n):
+    p, m = _cloud(n, 7 + n)
+    got = _run(p, m, 0.004, 1.0, 0)
+    ref = _oracle(p, m, 0.004, 1.0)
+    assert np.max(np.abs(got - ref)) <= 1e-12 * np.max(np.abs(ref))
+
+
+def test_mixed_pair_forces_conserve_momentum():
+    # each off-diagonal pair applies equal and opposite FP32 forces
+    p, m = _cloud(20001, 3)
+    got = _run(p, m, 0.004, 1.0, 1)
+    ma = got[:, :3] * m[:, None]
+    assert np.linalg.norm(ma.sum(0)) < 1e-6 * np.abs(ma).sum()
