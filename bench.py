@@ -207,6 +207,38 @@ def adjoint_cost(steps=3, warmup=3):
     return out
 
 
+def energy_drift(n, steps):
+    """Energy conservation over `steps` steps of the bench workload at N = n:
+    the mixed form and the FP64 form run side by side from the same initial
+    conditions (the FP64 GPU step equals the FP64 oracle to 1e-12 per kernel
+    and 1e-8 over whole steps in the parity tests; the oracle itself cannot
+    run N = 1M steps in bounded time).  Reported: each form's relative drift
+    (E_K - E_0) / |E_0|, and the largest |E_mixed - E_fp64| / |E_0| over the
+    run (same step index; the two forms' timesteps differ by rounding only).
+    The energy is a by-product of each step's force pass, so E_0 is the energy
+    after the first step and the K steps follow it."""
+    import time
+    from cudasph_b200.simulation import Simulation, make_params
+    ic = workload_ic(n)
+    res = {"workload": workload_name(n), "steps": steps}
+    E = {}
+    for name, prec in (("fp64", 0), ("mixed", 1)):
+        s = Simulation(ic, make_params(**dict(WORKLOAD_PARAMS, precision=prec)))
+        e, t0 = [], time.perf_counter()
+        s.step()
+        e0 = s.system_statistics()["E"]
+        for _ in range(steps):
+            s.step()
+            e.append(s.system_statistics()["E"])
+        s.synchronize()
+        E[name] = np.array(e)
+        res[name] = {"E0": e0, "E_end": e[-1], "drift_rel": (e[-1] - e0) / abs(e0), "t_end": s.time,
+                     "wall_s": time.perf_counter() - t0, "device_flags": s.device_status()}
+        s.close()
+    res["mixed_vs_fp64_max_rel"] = float(np.max(np.abs(E["mixed"] - E["fp64"])) / abs(res["fp64"]["E0"]))
+    return res
+
+
 def cpu_reference_sample(ic, n_grav_targets=256):
     from oracle import oracle as O
     if not O.ref_available():
@@ -414,7 +446,12 @@ def main():
     ap.add_argument("--cpu-grav-targets", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false")
+    ap.add_argument("--drift-steps", type=int, default=0,
+                    help="instead of the bench line, measure energy drift over this many steps (mixed vs FP64)")
     args = ap.parse_args()
+    if args.drift_steps > 0:
+        print(json.dumps({"measurement": "energy_drift", **energy_drift(args.n, args.drift_steps)}), flush=True)
+        return
     assert args.warmup >= 3 or args.impl == "reference" or os.environ.get("BENCH_ALLOW_SHORT_WARMUP")
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

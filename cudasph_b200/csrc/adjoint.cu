@@ -170,10 +170,16 @@ __global__ void k_adj_timestep(AdjArgs a, int nb_kick, int nb_min) {
   const double gv = isfinite(dtv) ? dtb1 * tau * tau / (dtv * dtv) : 0.0;  // dL/d dtv
   const double ge = isfinite(dte) ? dtb1 * tau * tau / (dte * dte) : 0.0;  // dL/d dte
   const double sw = (w / vs) >= 0 ? 1.0 : -1.0, se = (up / du) >= 0 ? 1.0 : -1.0;
-  a.xb[idx].w += gv * a.cn1 * sw / vs;
-  a.asc[2] = -gv * a.cn1 * sw * w / (vs * vs);
-  a.vpb[idx].w += ge * a.cn2 * se / du;
-  a.ab[idx].w += -ge * a.cn2 * se * up / (du * du);
+  // a limit that is not active (du = 0 gives dte = inf) passes no adjoint; its
+  // terms would be 0 * inf
+  if (gv != 0) {
+    a.xb[idx].w += gv * a.cn1 * sw / vs;
+    a.asc[2] = -gv * a.cn1 * sw * w / (vs * vs);
+  }
+  if (ge != 0) {
+    a.vpb[idx].w += ge * a.cn2 * se / du;
+    a.ab[idx].w += -ge * a.cn2 * se * up / (du * du);
+  }
 }
 
 // -- 5. gravity VJP: xbar_i += sum_j T_ij (m_i gbar_j - m_j gbar_i) ----------
