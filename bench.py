@@ -239,6 +239,74 @@ def energy_drift(n, steps):
     return res
 
 
+LARGE_N = 1 << 22
+LARGE_PARAMS = dict(n_target=50.0, eos_mode=0, soft_mode=1, eps=0.001)
+
+
+def large_run(n=LARGE_N, steps=5, n_sub=262144):
+    """The gravity-dominated workload: N = 4,194,304 cold uniform-density
+    sphere (virial ratio 0.1, u = 1e-6, seeded positions), ideal gas,
+    N_ngb = 50, Plummer eps = 0.001; `steps` mixed-precision steps (device
+    time per phase, CUDA events; the first step solves h from the initial
+    guess), gravity interactions/s against the FP32 FMA peak measured in the
+    same run; then one adjoint step (gravity + hydro forces and the rest of
+    the step) on a seeded 262,144-particle subset of the same sphere (masses
+    scaled so the subset keeps the total mass)."""
+    from cudasph_b200 import ics, _capi
+    from cudasph_b200.simulation import Simulation, make_params
+    L = _capi.lib()
+    peak32 = L.cudasph_fma_peak(1, 4096, None)
+    ic = ics.cold_sphere(n, virial=0.1, u0=1e-6, n_ngb=50.0, seed=12345 + 5)
+    res = {"workload": f"cold uniform sphere, N={n}, virial 0.1, u=1e-6, ideal gas, N_ngb=50, Plummer eps=0.001, "
+                       f"mixed precision", "steps": steps}
+    sim = Simulation(ic, make_params(precision=1, **LARGE_PARAMS))
+    sim.reset_counters()
+    sim.set_profiling(True)
+    sim.step(steps)
+    sim.synchronize()
+    ph = sim.phase_times()
+    sim.set_profiling(False)
+    gms = ph["gravity"][0] / steps
+    step_ms = sum(v[0] for v in ph.values()) / steps
+    res["ms_per_step"] = step_ms
+    res["particle_steps_per_s"] = n / (step_ms * 1e-3)
+    res["phase_ms_per_step"] = {k: round(v[0] / steps, 3) for k, v in ph.items()}
+    res["gravity"] = {"ms_per_launch": gms, "interactions_per_s": n * n / (gms * 1e-3),
+                      "tflops_at_20_per_interaction": 20.0 * n * n / (gms * 1e-3) / 1e12,
+                      "fp32_fma_peak_tflops": peak32 / 1e12,
+                      "frac_of_fp32_peak": 20.0 * n * n / (gms * 1e-3) / peak32}
+    res["stats_last_step"] = {k: v for k, v in sim.system_statistics().items() if k in ("E", "dt", "ngb_mean")}
+    res["device_flags"] = sim.device_status()
+    sim.close()
+
+    rng = np.random.default_rng(12345 + 5)
+    idx = np.sort(rng.choice(n, n_sub, replace=False))
+    sub = {k: (np.asarray(v)[idx].copy() if isinstance(v, np.ndarray) else v) for k, v in ic.items()}
+    sub["m"] = sub["m"] * (n / n_sub)
+    rho = np.full(n_sub, 3.0 / (4.0 * math.pi))
+    sub["range"] = ics.initial_range(rho, sub["m"], 50.0)
+    s2 = Simulation(sub, make_params(precision=1, **LARGE_PARAMS))
+    s2.set_keep(True)
+    s2.step(3)
+    s2.synchronize()
+    s2.reset_counters()
+    s2.set_profiling(True)
+    s2.step()
+    m = sub["m"]
+    for k in ("vx", "vy", "vz"):
+        s2.adjoint_set(k, m * s2.get(k))
+    s2.adjoint()
+    s2.synchronize()
+    ph2 = s2.phase_times()
+    s2.set_profiling(False)
+    fwd = sum(v[0] for k, v in ph2.items() if k != "adjoint")
+    adj = ph2["adjoint"][0]
+    res["adjoint_subset"] = {"n": n_sub, "forward_ms": fwd, "adjoint_ms": adj, "adjoint_over_forward": adj / fwd,
+                             "loss": "kinetic energy after the step", "device_flags": s2.device_status()}
+    s2.close()
+    return res
+
+
 def cpu_reference_sample(ic, n_grav_targets=256):
     from oracle import oracle as O
     if not O.ref_available():
@@ -448,7 +516,13 @@ def main():
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false")
     ap.add_argument("--drift-steps", type=int, default=0,
                     help="instead of the bench line, measure energy drift over this many steps (mixed vs FP64)")
+    ap.add_argument("--large", action="store_true",
+                    help="instead of the bench line, run the N = 4,194,304 cold-sphere workload (5 steps + a subset "
+                         "adjoint)")
     args = ap.parse_args()
+    if args.large:
+        print(json.dumps({"measurement": "large_cold_sphere", **large_run()}), flush=True)
+        return
     if args.drift_steps > 0:
         print(json.dumps({"measurement": "energy_drift", **energy_drift(args.n, args.drift_steps)}), flush=True)
         return
