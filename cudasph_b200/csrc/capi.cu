@@ -229,7 +229,7 @@ extern "C" sph_params cudasph_default_params(void) {
   p.precision = SPH_PREC_FP64;
   p.ngb_cap = 0;
   p.sort_every = 1;
-  p.mixed_sph = 3;
+  p.mixed_sph = 0;
   return p;
 }
 

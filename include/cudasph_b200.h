@@ -73,7 +73,11 @@ typedef struct {
   int ngb_cap;       /* neighbour-list capacity per particle (0 = 4 * n_target + 32) */
   int sort_every;    /* Morton re-sort period in steps (reference: 100, step.cpp:26) */
   int mixed_sph;     /* mixed form only: bit 0 = density pair terms in FP32, bit 1 = hydro
-                        pair terms in FP32 (default 3); a cleared bit keeps that loop in FP64 */
+                        pair terms in FP32; a cleared bit keeps that loop in FP64.  Default 0:
+                        the SPH loops are gather-bound, so FP64 pair terms cost ~0.5 % of a
+                        1M-particle step, while FP32 ones raise the RMS total-force error of a
+                        star near hydrostatic equilibrium (hydro and gravity nearly cancel)
+                        from 4.9e-7 to 2.2e-5 */
 } sph_params;
 
 /* particle fields, addressed in the caller's ORIGINAL particle order */

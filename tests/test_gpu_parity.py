@@ -165,6 +165,24 @@ def test_gravity_mixed_accuracy(poly, soft):
     assert _rel(sim.get("phi"), ref[3]) < 1e-5
 
 
+@pytest.mark.parametrize("mask", [1, 2, 3])
+def test_mixed_sph_pair_terms(poly, mask):
+    """The FP32 density (bit 0) and hydro (bit 1) pair loops of the mixed
+    form, against the FP64 step at the same state."""
+    kw = dict(n_target=50.0, eos_mode=1, soft_mode=1, eps=0.01)
+    a = _sim(poly, precision=1, mixed_sph=mask, **kw)
+    b = _sim(poly, **kw)
+    a.step()
+    b.step()
+    assert np.max(np.abs(a.get("rho") / b.get("rho") - 1)) < (1e-6 if mask & 1 else 1e-12)
+    ha = np.stack([a.get(k) - a.get(g) for k, g in (("ax", "gx"), ("ay", "gy"), ("az", "gz"))], 1)
+    hb = np.stack([b.get(k) - b.get(g) for k, g in (("ax", "gx"), ("ay", "gy"), ("az", "gz"))], 1)
+    rms = np.sqrt(np.mean(np.sum((ha - hb) ** 2, 1)) / np.mean(np.sum(hb ** 2, 1)))
+    assert rms < 1e-5, rms
+    assert _rel(a.get("du"), b.get("du")) < 1e-4
+    assert a.device_status() & 0x7 == 0
+
+
 def test_whole_steps_fp64_match_oracle():
     ic = ics.polytrope(3000, n_ngb=50, seed=3)
     kw = dict(n_target=50.0, eos_mode=0, soft_mode=1, eps=0.01)
