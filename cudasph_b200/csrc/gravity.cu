@@ -422,9 +422,11 @@ __global__ void __launch_bounds__(kGThreads) k_grav_f32x2_plummer(int n, const d
 // ------------------ mixed (FP32), symmetric pair form -----------------------
 // Plummer gravity computing each pair once (Newton's third law): the force
 // of a pair is applied to i and, with the opposite sign and i's mass, to j.
-// Per two pairs (one packed i-pair against one j) the loop issues 19 packed
-// FP32 instructions and 2 MUFU.rsq, against 26 and 4 when both directions
-// are computed separately.
+// Per two pairs (one packed i-pair against one j) the loop issues 18 packed
+// FP32 instructions (3 sub, 3 FMA for s^2, 2 mul for s^-3, 2 mul for the
+// mass-weighted s^-3 of each side, 2 x 4 FMA into the i- and j-side sums)
+// and 2 MUFU.rsq, against 26 and 4 when both directions are computed
+// separately.
 //
 // Work split: the Morton order is cut into tiles of kSymTile particles; a
 // block owns one i-tile (kSymWarps warps, kSymRP packed i-pairs per lane) and
@@ -520,14 +522,14 @@ __global__ void __launch_bounds__(kSymWarps * 32, 4) k_grav_sym_plummer(int n, i
         upk2(r2, r2a, r2b);
         const f32x2 inv = pk2(rsqrt_f32(r2a), rsqrt_f32(r2b));
         const f32x2 inv3 = mul2(mul2(inv, inv), inv);
-        const f32x2 qx = mul2(dx, inv3), qy = mul2(dy, inv3), qz = mul2(dz, inv3);
-        px[p] = fma2(MJ, qx, px[p]);
-        py[p] = fma2(MJ, qy, py[p]);
-        pz[p] = fma2(MJ, qz, pz[p]);
+        const f32x2 sj = mul2(MJ, inv3), si = mul2(nmi[p], inv3);  // m_j / s^3, -m_i / s^3
+        px[p] = fma2(dx, sj, px[p]);
+        py[p] = fma2(dy, sj, py[p]);
+        pz[p] = fma2(dz, sj, pz[p]);
         pp[p] = fma2(MJ, inv, pp[p]);
-        AX = fma2(nmi[p], qx, AX);
-        AY = fma2(nmi[p], qy, AY);
-        AZ = fma2(nmi[p], qz, AZ);
+        AX = fma2(dx, si, AX);
+        AY = fma2(dy, si, AY);
+        AZ = fma2(dz, si, AZ);
         AP = fma2(nmi[p], inv, AP);
       }
       float a0, a1;
