@@ -20,7 +20,7 @@ int morton_keys(int n, const double4 *pos, const double *x, const double *y, con
 int tree_layout(int n, TreeView *t);
 int build_tree(const TreeView &t, const double4 *pos, float4 *lo, float4 *hi, cudaStream_t st);
 int launch_solve_range(const TreeView &t, double4 *pos, int *nevals, unsigned *flags, const sph_params &p,
-                       int *n_ngb, int *list, int cap, cudaStream_t st);
+                       int *n_ngb, int *list, double *dcache, int cap, cudaStream_t st);
 int launch_find_ngb(const TreeView &t, const double4 *pos, int *n_ngb, int *list, int cap, unsigned *flags,
                     cudaStream_t st);
 int launch_density(const HydroArgs &a, cudaStream_t st);
@@ -73,6 +73,7 @@ struct sph_ctx {
   double4 *old = nullptr;
   int *n_ngb = nullptr, *nevals = nullptr, *list = nullptr;
   int list_cap = 0;  // per particle
+  double *dcache = nullptr;  // candidate squared distances of the h solve, layout of list
   TreeView tree;
   float4 *tlo = nullptr, *thi = nullptr;
   uint64_t *keys = nullptr;
@@ -152,11 +153,15 @@ int alloc_lists(sph_ctx *c) {
   int cap = c->p.ngb_cap > 0 ? c->p.ngb_cap : (int)(4 * c->p.n_target) + 32;
   if (cap == c->list_cap && c->list) return SPH_OK;
   if (c->list) cudaFree(c->list);
+  if (c->dcache) cudaFree(c->dcache);
   c->list = nullptr;
+  c->dcache = nullptr;
   c->list_cap = cap;
   size_t entries = (size_t)c->tree.count[0] * kLeaf * (size_t)cap;
   c->lists_ok = false;
-  return dalloc(&c->list, entries);
+  int rc = dalloc(&c->list, entries);
+  if (!rc) rc = dalloc(&c->dcache, entries);
+  return rc;
 }
 
 int check_params(const sph_params *p) {
@@ -242,7 +247,7 @@ extern "C" int cudasph_destroy(sph_ctx *c) {
     cudaFree(F.pos); cudaFree(F.vel); cudaFree(F.hyd); cudaFree(F.dd); cudaFree(F.dots); cudaFree(F.grav);
     cudaFree(F.vsig); cudaFree(F.id);
   }
-  cudaFree(c->old); cudaFree(c->n_ngb); cudaFree(c->nevals); cudaFree(c->list);
+  cudaFree(c->old); cudaFree(c->n_ngb); cudaFree(c->nevals); cudaFree(c->list); cudaFree(c->dcache);
   cudaFree(c->tlo); cudaFree(c->thi); cudaFree(c->keys); cudaFree(c->vals); cudaFree(c->sort_scratch);
   cudaFree(c->bbox_part); cudaFree(c->box4); cudaFree(c->gsrc); cudaFree(c->gh2); cudaFree(c->flags);
   cudaFree(c->sc); cudaFree(c->fin_part); cudaFree(c->flat); cudaFree(c->slot_of);
@@ -551,8 +556,8 @@ extern "C" int cudasph_solve_range(sph_ctx *c) {
   }
   SPH_CUDA_TRY(cudaSetDevice(c->device));
   PhaseScope ps(c, SPH_PH_SOLVE);
-  LAUNCHED(launch_solve_range(c->tree, c->f[c->cur].pos, c->nevals, c->flags, c->p, c->n_ngb, c->list, c->list_cap,
-                              c->st));
+  LAUNCHED(launch_solve_range(c->tree, c->f[c->cur].pos, c->nevals, c->flags, c->p, c->n_ngb, c->list, c->dcache,
+                              c->list_cap, c->st));
   // the solve writes the neighbour lists at the final ranges (find_ngb fused)
   c->lists_ok = true;
   c->density_ok = false;

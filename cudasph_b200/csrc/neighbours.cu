@@ -158,18 +158,34 @@ struct SolveArgs {
   unsigned *flags;
   double n_target, rel_err, f_scale;
   int max_iter;
-  int *n_ngb;  // hard count at the final range
-  int *list;   // neighbour lists at the final range (layout of k_find_ngb)
+  int *n_ngb;      // hard count at the final range
+  int *list;       // neighbour lists at the final range (layout of k_find_ngb)
+  double *dcache;  // squared distances of the cached candidates, layout of list
   int cap;
 };
 
 enum { kBr0 = 0, kBr1 = 1, kSolve = 2, kDone = 3 };
 
+// radius of a candidate cache relative to the range that fills it: one
+// clamped Newton step of the bracket (f_scale = 10 %) stays inside it
+constexpr double kCacheMargin = 1.15;
+
 // dev_solve_range (dev_solve_range.cu:137-189): per particle, bracket the
 // root of f(w) = sum_j ig(2 r_ij / w) - N_target with clamped Newton steps
 // (dev_bracket_root :93-135), then safeguarded Newton / bisection until
-// |dx| < rel_err * w.  Each lane runs that iteration as a state machine; the
-// lanes that need an evaluation of f in a round share one tree walk.
+// |dx| < rel_err * w.  Each lane runs that iteration as a state machine.
+//
+// Candidate cache (find_ngb fused in): a lane whose range w is not covered
+// by its cache walks the tree once at radius 1.15 w and stores every j with
+// d2 < (1.15 w)^2 -- index in its column of the neighbour list, exact FP64
+// d2 in the same column of dcache -- in the walk's ascending order.  Every
+// evaluation of f (and of its derivative) then runs over the cached entries
+// with d2 < w^2 in that order, the same operations in the same order as a
+// walk at w, and the final list is the cache compacted in place to the final
+// range.  The lanes that need a walk in a round share it.  A lane whose
+// candidates exceed the list capacity falls back to walking at w for every
+// evaluation, writing its list as it goes (`direct`), with one list-only walk
+// when the final range differs from the last one evaluated (`pending`).
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_solve_range(SolveArgs a) {
   __shared__ WarpSmem smem[kWarpsPerBlock];
   WarpSmem &sm = smem[threadIdx.x >> 5];
@@ -189,52 +205,81 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_solve_range(SolveArgs a
   int iter = 0, keep = 0, nev = 0;
   bool stack_ok = true;
   const double rel = a.rel_err, fs = a.f_scale;
-  // Every evaluation also writes the lane's neighbour list at the range it
-  // evaluates (find_ngb fused in): the final range is the last one evaluated,
-  // except when the bracket converges at once and the midpoint of
-  // (w - |dx|/2, w + |dx|/2) rounds away from w -- then one list-only round
-  // at the final range follows (`pending`).
-  int *out = a.list + (size_t)leaf * a.cap * kLeaf + lane_id();
+  const size_t col = (size_t)leaf * a.cap * kLeaf + lane_id();
+  int *lst = a.list + col;
+  double *dc = a.dcache + col;
   const int cap = a.cap;
-  double w_list = -1.0;
+  int ncache = 0;           // cached entries
+  double cache_r2 = -1.0;   // the cache holds every j with d2 < cache_r2
+  bool direct = false;
+  double w_list = -1.0;     // direct lanes: range of the list last written
   int cnt_list = 0;
   bool pending = false;
   while (true) {
     const bool iterate = phase != kDone;
-    const bool need = iterate || pending;
-    if (!__any_sync(kFull, need)) break;
-    float ql[3], qh[3];
-    warp_query_box(need, xi, yi, zi, w, ql, qh);
-    double sf = 0, sg = 0;
-    int c = 0;
+    if (!__any_sync(kFull, iterate || pending)) break;
     const double w2 = __dmul_rn(w, w);
-    const float thr = prefilter_threshold(pf, w);
-    stack_ok &= walk_leaves(a.t, ql, qh, sm.stack, [&](int lj) {
-      stage_leaf(a.pos, n, lj, sm, pf);
-      const int cntj = min(kLeaf, n - lj * kLeaf);
-      if (need) {
-        for (int k = 0; k < cntj; k++) {
-          if (certainly_outside(pf, thr, sm.sf[k])) continue;
-          const double d2 = ds2_exact(xi - sm.sx[k], yi - sm.sy[k], zi - sm.sz[k]);
-          if (d2 < w2) {
-            if (c < cap) out[(size_t)c * kLeaf] = lj * kLeaf + k;
-            c++;
-            if (iterate) {
-              const double u = 2 * sqrt(d2) / w;
-              sf += k_ig<double>(u);
-              sg -= k_digdh<double>(u);
+    const bool fill = iterate && !direct && !(w2 <= cache_r2);
+    const bool dwalk = (iterate && direct) || pending;
+    double sf = 0, sg = 0;
+    bool evaluated = false;
+    if (__any_sync(kFull, fill || dwalk)) {
+      const bool on = fill || dwalk;
+      const double r = fill ? w * kCacheMargin : w;
+      const double r2 = __dmul_rn(r, r);
+      float ql[3], qh[3];
+      warp_query_box(on, xi, yi, zi, r, ql, qh);
+      const float thr = prefilter_threshold(pf, r);
+      int c = 0;
+      stack_ok &= walk_leaves(a.t, ql, qh, sm.stack, [&](int lj) {
+        stage_leaf(a.pos, n, lj, sm, pf);
+        const int cntj = min(kLeaf, n - lj * kLeaf);
+        if (on) {
+          for (int k = 0; k < cntj; k++) {
+            if (certainly_outside(pf, thr, sm.sf[k])) continue;
+            const double d2 = ds2_exact(xi - sm.sx[k], yi - sm.sy[k], zi - sm.sz[k]);
+            if (d2 < r2) {
+              if (c < cap) {
+                lst[(size_t)c * kLeaf] = lj * kLeaf + k;
+                if (fill) dc[(size_t)c * kLeaf] = d2;
+              }
+              c++;
+              if (dwalk && iterate) {
+                const double u = 2 * sqrt(d2) / w;
+                sf += k_ig<double>(u);
+                sg -= k_digdh<double>(u);
+              }
             }
           }
         }
+      });
+      if (fill) {
+        if (c <= cap) {
+          ncache = c;
+          cache_r2 = r2;
+        } else {
+          direct = true;  // evaluated by a walk at w from the next round on
+        }
       }
-    });
-    if (!need) continue;
-    w_list = w;
-    cnt_list = c;
-    if (!iterate) {
-      pending = false;
-      continue;
+      if (dwalk) {
+        w_list = w;
+        cnt_list = c;
+        if (iterate) evaluated = true;
+        else pending = false;
+      }
     }
+    if (iterate && !direct && w2 <= cache_r2) {
+      for (int k = 0; k < ncache; k++) {
+        const double d2 = dc[(size_t)k * kLeaf];
+        if (d2 < w2) {
+          const double u = 2 * sqrt(d2) / w;
+          sf += k_ig<double>(u);
+          sg -= k_digdh<double>(u);
+        }
+      }
+      evaluated = true;
+    }
+    if (!evaluated) continue;
     nev++;
     // compute_ngb epilogue, dev_solve_range.cu:77-87
     f = sf - a.n_target;
@@ -299,7 +344,26 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_solve_range(SolveArgs a
         phase = kDone;
       }
     }
-    pending = (phase == kDone) && (w != w_list);
+    if (phase == kDone) {
+      if (direct) {
+        pending = w != w_list;
+      } else if (!(__dmul_rn(w, w) <= cache_r2)) {
+        direct = true;  // final range outside the cache: list by a walk
+        pending = true;
+      }
+    }
+  }
+  if (valid && !direct && cache_r2 >= 0) {
+    // the final list: the cached entries inside the final range, in order
+    const double w2 = __dmul_rn(w, w);
+    int c = 0;
+    for (int k = 0; k < ncache; k++) {
+      if (dc[(size_t)k * kLeaf] < w2) {
+        lst[(size_t)c * kLeaf] = lst[(size_t)k * kLeaf];
+        c++;
+      }
+    }
+    cnt_list = c;
   }
   if (!stack_ok && lane_id() == 0) raise_flag(a.flags, SPH_FLAG_STACK_OVERFLOW);
   if (cnt_list > cap) raise_flag(a.flags, SPH_FLAG_NGB_OVERFLOW);
@@ -368,10 +432,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_find_ngb(FindArgs a) {
 }
 
 int launch_solve_range(const TreeView &t, double4 *pos, int *nevals, unsigned *flags, const sph_params &p,
-                       int *n_ngb, int *list, int cap, cudaStream_t st) {
+                       int *n_ngb, int *list, double *dcache, int cap, cudaStream_t st) {
   SolveArgs a;
   a.t = t; a.pos = pos; a.nevals = nevals; a.flags = flags;
-  a.n_ngb = n_ngb; a.list = list; a.cap = cap;
+  a.n_ngb = n_ngb; a.list = list; a.dcache = dcache; a.cap = cap;
   a.n_target = p.n_target; a.rel_err = p.rel_err; a.f_scale = p.f_scale; a.max_iter = p.max_iter;
   const int warps = t.count[0];
   k_solve_range<<<(warps + kWarpsPerBlock - 1) / kWarpsPerBlock, kWarpsPerBlock * 32, 0, st>>>(a);
