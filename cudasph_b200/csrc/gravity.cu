@@ -96,14 +96,19 @@ __device__ __noinline__ void spline_near(R dx, R dy, R dz, R r2, R mj, R hi2, R 
 }
 
 // -------------------------------- FP64 --------------------------------------
+// One-sided form: every i of the block against the sources [jlo, jhi); with
+// tile > 0 the range is the tile of `tile` particles that holds the block
+// (the diagonal tiles of the symmetric form), else all n.
 template <int SOFT, int R>
 __global__ void __launch_bounds__(kGThreads) k_grav_f64(int n, const double4 *__restrict__ src,
                                                         const double *__restrict__ h2src, double4 *__restrict__ out,
-                                                        double eps2, double G) {
+                                                        double eps2, double G, int tile) {
   __shared__ double4 sj[kGThreads];
   __shared__ double sh[SOFT == SPH_SOFT_SPLINE ? kGThreads : 1];
   const int t = threadIdx.x;
   const int i0 = blockIdx.x * kGThreads * R;
+  const int jlo = tile > 0 ? (i0 / tile) * tile : 0;
+  const int jhi = tile > 0 ? min(jlo + tile, n) : n;
   double xi[R], yi[R], zi[R], hi2[R], ax[R], ay[R], az[R], pot[R];
 #pragma unroll
   for (int r = 0; r < R; r++) {
@@ -113,15 +118,15 @@ __global__ void __launch_bounds__(kGThreads) k_grav_f64(int n, const double4 *__
     hi2[r] = (SOFT == SPH_SOFT_SPLINE) ? h2src[i] : 0.0;
     ax[r] = ay[r] = az[r] = pot[r] = 0.0;
   }
-  for (int j0 = 0; j0 < n; j0 += kGThreads) {
+  for (int j0 = jlo; j0 < jhi; j0 += kGThreads) {
     const int j = j0 + t;
     __syncthreads();
-    if (j < n) {
+    if (j < jhi) {
       sj[t] = src[j];
       if (SOFT == SPH_SOFT_SPLINE) sh[t] = h2src[j];
     }
     __syncthreads();
-    const int m = min(kGThreads, n - j0);
+    const int m = min(kGThreads, jhi - j0);
     if (SOFT == SPH_SOFT_PLUMMER) {
 #pragma unroll 4
       for (int k = 0; k < m; k++) {
@@ -582,6 +587,103 @@ __global__ void __launch_bounds__(kSymWarps * 32, 4) k_grav_sym_plummer(int n, i
   }
 }
 
+// ------------------- FP64, symmetric pair form ------------------------------
+// The plain form of the symmetric Plummer kernel above: the same tiles, work
+// items, travelling sources and block-combined j-side atomics, in FP64 with
+// absolute coordinates (no anchor), kSym64R i-particles per lane and their
+// FP64 sums in registers for the whole item.  Per pair: 3 sub, 3 FMA for
+// s^2, the FP64 rsqrt (MUFU seed + one Householder step: 5 FP64 ops),
+// 2 mul for s^-3, 2 for the mass-weighted s^-3 of each side, 8 FMA into the
+// i- and j-side sums -- 23 FP64 operations against 36 for both directions.
+constexpr int kSym64Warps = 4;
+constexpr int kSym64R = 8;
+static_assert(kSym64Warps * 32 * kSym64R == kSymTile, "the FP64 form shares the tile layout");
+
+__global__ void __launch_bounds__(kSym64Warps * 32) k_grav_sym_f64(int n, int nt, const double4 *__restrict__ src,
+                                                                  double4 *__restrict__ out, double eps2, double G) {
+  __shared__ double red[2][kSym64Warps][4][32];
+  const long long item = blockIdx.x;
+  int lo = 0, hi = nt - 2;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (sym_first(mid, nt) <= item) lo = mid; else hi = mid - 1;
+  }
+  const int b = lo;
+  const int t_lo = b + 1 + (int)(item - sym_first(b, nt)) * kSymChunk;
+  const int t_hi = min(t_lo + kSymChunk, nt);
+  const int j_lo = t_lo * kSymTile, j_hi = min(t_hi * kSymTile, n);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nxt = (l + 1) & 31;
+  const int ib = b * kSymTile + w * 32 * kSym64R + l;
+  const double4 far = src[b * kSymTile];  // position given to padding i-slots
+
+  double xi[kSym64R], yi[kSym64R], zi[kSym64R], nmi[kSym64R];
+  double ax[kSym64R], ay[kSym64R], az[kSym64R], ap[kSym64R];
+#pragma unroll
+  for (int r = 0; r < kSym64R; r++) {
+    const int i = ib + r * 32;
+    const double4 q = i < n ? src[i] : make_double4(far.x, far.y, far.z, 0.0);
+    xi[r] = q.x; yi[r] = q.y; zi[r] = q.z; nmi[r] = -q.w;
+    ax[r] = ay[r] = az[r] = ap[r] = 0.0;
+  }
+  int k = 0;
+  for (int jb = j_lo; jb < j_hi; jb += 32, k ^= 1) {
+    // padding source: massless, at a real position of the i-tile (s^2 >= eps^2 > 0)
+    const double4 q = (jb + l < j_hi) ? src[jb + l] : make_double4(far.x, far.y, far.z, 0.0);
+    double xj = q.x, yj = q.y, zj = q.z, mj = q.w;
+    double bx = 0.0, by = 0.0, bz = 0.0, bp = 0.0;
+#pragma unroll 1
+    for (int s = 0; s < 32; s++) {
+#pragma unroll
+      for (int r = 0; r < kSym64R; r++) {
+        const double dx = xj - xi[r], dy = yj - yi[r], dz = zj - zi[r];
+        const double r2 = fma(dz, dz, fma(dy, dy, fma(dx, dx, eps2)));
+        const double inv = rsqrt_f64(r2);
+        const double inv3 = inv * inv * inv;
+        const double sj = mj * inv3, si = nmi[r] * inv3;  // m_j / s^3, -m_i / s^3
+        ax[r] = fma(dx, sj, ax[r]);
+        ay[r] = fma(dy, sj, ay[r]);
+        az[r] = fma(dz, sj, az[r]);
+        ap[r] = fma(-mj, inv, ap[r]);
+        bx = fma(dx, si, bx);
+        by = fma(dy, si, by);
+        bz = fma(dz, si, bz);
+        bp = fma(nmi[r], inv, bp);
+      }
+      xj = __shfl_sync(0xffffffffu, xj, nxt);
+      yj = __shfl_sync(0xffffffffu, yj, nxt);
+      zj = __shfl_sync(0xffffffffu, zj, nxt);
+      mj = __shfl_sync(0xffffffffu, mj, nxt);
+      bx = __shfl_sync(0xffffffffu, bx, nxt);
+      by = __shfl_sync(0xffffffffu, by, nxt);
+      bz = __shfl_sync(0xffffffffu, bz, nxt);
+      bp = __shfl_sync(0xffffffffu, bp, nxt);
+    }
+    red[k][w][0][l] = bx;
+    red[k][w][1][l] = by;
+    red[k][w][2][l] = bz;
+    red[k][w][3][l] = bp;
+    __syncthreads();  // also orders this batch's reads of red[k] before batch + 2 writes it
+    for (int qq = threadIdx.x; qq < 128; qq += kSym64Warps * 32) {
+      const int c = qq >> 5, ll = qq & 31;
+      double sum = 0.0;
+#pragma unroll
+      for (int v = 0; v < kSym64Warps; v++) sum += red[k][v][c][ll];
+      if (jb + ll < j_hi) atomicAdd(&reinterpret_cast<double *>(out + jb + ll)[c], G * sum);
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < kSym64R; r++) {
+    const int i = ib + r * 32;
+    if (i < n) {
+      double *o = reinterpret_cast<double *>(out + i);
+      atomicAdd(o + 0, G * ax[r]);
+      atomicAdd(o + 1, G * ay[r]);
+      atomicAdd(o + 2, G * az[r]);
+      atomicAdd(o + 3, G * ap[r]);
+    }
+  }
+}
+
 // src = {x, y, z, m} per particle; h2src = range^2 (spline mode only)
 int launch_gravity(int n, const double4 *src, const double *h2src, double4 *out, int soft_mode, double eps, double G,
                    int precision, cudaStream_t st) {
@@ -589,11 +691,19 @@ int launch_gravity(int n, const double4 *src, const double *h2src, double4 *out,
   const double eps2 = eps * eps;
   if (precision == SPH_PREC_FP64) {
     constexpr int R = 2;
+    static_assert(kSymTile % (kGThreads * R) == 0, "diagonal tiles must hold whole blocks");
     const int blocks = (n + kGThreads * R - 1) / (kGThreads * R);
-    if (soft_mode == SPH_SOFT_PLUMMER)
-      k_grav_f64<SPH_SOFT_PLUMMER, R><<<blocks, kGThreads, 0, st>>>(n, src, h2src, out, eps2, G);
-    else
-      k_grav_f64<SPH_SOFT_SPLINE, R><<<blocks, kGThreads, 0, st>>>(n, src, h2src, out, eps2, G);
+    const int nt = (n + kSymTile - 1) / kSymTile;
+    if (soft_mode == SPH_SOFT_PLUMMER) {
+      if (nt < 2) {
+        k_grav_f64<SPH_SOFT_PLUMMER, R><<<blocks, kGThreads, 0, st>>>(n, src, h2src, out, eps2, G, 0);
+      } else {
+        k_grav_f64<SPH_SOFT_PLUMMER, R><<<blocks, kGThreads, 0, st>>>(n, src, h2src, out, eps2, G, kSymTile);
+        k_grav_sym_f64<<<(unsigned)sym_S(nt - 1), kSym64Warps * 32, 0, st>>>(n, nt, src, out, eps2, G);
+      }
+    } else {
+      k_grav_f64<SPH_SOFT_SPLINE, R><<<blocks, kGThreads, 0, st>>>(n, src, h2src, out, eps2, G, 0);
+    }
   } else {
     if (soft_mode == SPH_SOFT_PLUMMER) {
       // one i-pair per thread measured fastest at N = 1M (68 registers, more
