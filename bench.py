@@ -174,7 +174,7 @@ ADJOINT_N = 65536
 ADJOINT_PARAMS = dict(n_target=50.0, eos_mode=1, soft_mode=1, eps=0.01)
 
 
-def adjoint_cost(steps=3, warmup=3):
+def adjoint_cost(steps=3, warmup=3, headline_n=None):
     """Cost of the hand-written adjoint of one step relative to the forward
     step, on the differentiation workload: an n=3 polytrope, N = 65,536,
     ideal gas + radiation EOS, N_ngb = 50, Plummer eps = 0.01.  Device time
@@ -185,12 +185,19 @@ def adjoint_cost(steps=3, warmup=3):
     from cudasph_b200.simulation import Simulation, make_params
     ic = ics.polytrope(ADJOINT_N, n_poly=3.0, n_ngb=50.0, seed=12345 + 4, mu=0.62)
     out = {"workload": f"n=3 polytrope, N={ADJOINT_N}, gas+radiation EOS mu=0.62, N_ngb=50, Plummer eps=0.01"}
+    def step_and_adjoint(sim, m):
+        sim.step()
+        for k in ("vx", "vy", "vz"):
+            sim.adjoint_set(k, m * sim.get(k))
+        sim.adjoint()
+
     for name, prec in (("fp64", 0), ("mixed", 1)):
         sim = Simulation(ic, make_params(precision=prec, **ADJOINT_PARAMS))
         sim.set_keep(True)
-        sim.step(warmup)
-        sim.synchronize()
         m = ic["m"]
+        for _ in range(warmup):  # warm-up includes the reverse sweep (first use of its kernels)
+            step_and_adjoint(sim, m)
+        sim.synchronize()
         sim.reset_counters()
         sim.set_profiling(True)
         for _ in range(steps):
@@ -204,6 +211,30 @@ def adjoint_cost(steps=3, warmup=3):
         adj = ph["adjoint"][0] / steps
         out[name] = {"forward_ms": fwd, "adjoint_ms": adj, "adjoint_over_forward": adj / fwd,
                      "replay_plus_adjoint_over_forward": (fwd + adj) / fwd, "flags": sim.device_status()}
+        sim.close()
+    if headline_n:
+        # the same ratio on the headline workload (mixed form, one step)
+        ic = workload_ic(headline_n)
+        sim = Simulation(ic, make_params(**dict(WORKLOAD_PARAMS, precision=1)))
+        sim.set_keep(True)
+        for _ in range(2):
+            step_and_adjoint(sim, ic["m"])
+        sim.synchronize()
+        sim.reset_counters()
+        sim.set_profiling(True)
+        sim.step()
+        m = ic["m"]
+        for k in ("vx", "vy", "vz"):
+            sim.adjoint_set(k, m * sim.get(k))
+        sim.adjoint()
+        ph = sim.phase_times()
+        sim.set_profiling(False)
+        fwd = sum(v[0] for k, v in ph.items() if k != "adjoint")
+        adj = ph["adjoint"][0]
+        out["headline_workload_mixed"] = {"n": headline_n, "forward_ms": fwd, "adjoint_ms": adj,
+                                          "adjoint_over_forward": adj / fwd,
+                                          "replay_plus_adjoint_over_forward": (fwd + adj) / fwd,
+                                          "flags": sim.device_status()}
         sim.close()
     return out
 
@@ -288,12 +319,16 @@ def large_run(n=LARGE_N, steps=5, n_sub=262144):
     sub["range"] = ics.initial_range(rho, sub["m"], 50.0)
     s2 = Simulation(sub, make_params(precision=1, **LARGE_PARAMS))
     s2.set_keep(True)
-    s2.step(3)
+    m = sub["m"]
+    for _ in range(3):  # warm-up includes the reverse sweep
+        s2.step()
+        for k in ("vx", "vy", "vz"):
+            s2.adjoint_set(k, m * s2.get(k))
+        s2.adjoint()
     s2.synchronize()
     s2.reset_counters()
     s2.set_profiling(True)
     s2.step()
-    m = sub["m"]
     for k in ("vx", "vy", "vz"):
         s2.adjoint_set(k, m * s2.get(k))
     s2.adjoint()
@@ -434,7 +469,7 @@ def run_ours(args, rank, world):
 
     # --- adjoint / forward cost (the differentiation form) --------------------------
     if args.adjoint:
-        out["adjoint"] = adjoint_cost()
+        out["adjoint"] = adjoint_cost(headline_n=n)
 
     # --- end to end through the C ABI with host buffers ----------------------------
     if args.e2e_steps > 0:

@@ -21,6 +21,7 @@
 #include <cstdio>
 
 #include "common.cuh"
+#include "pairmath.cuh"
 #include "sph_math.cuh"
 
 namespace sph {
@@ -184,31 +185,32 @@ __global__ void k_adj_timestep(AdjArgs a, int nb_kick, int nb_min) {
 
 // -- 5. gravity VJP: xbar_i += sum_j T_ij (m_i gbar_j - m_j gbar_i) ----------
 // T_ij = I / s^3 - 3 d d^T / s^5, d = x_j - x_i, s^2 = |d|^2 + eps^2 (Plummer).
+// The pair term v = T_ij w_ij is antisymmetric (d -> -d leaves T, w_ji =
+// -w_ij), so xbar_j receives -v: the symmetric kernels compute each pair
+// once with the tiles, work items and travelling sources of the forward
+// symmetric kernels (gravity.cu), and the one-sided kernels cover the
+// diagonal tiles (tile > 0) or all pairs of a small system (tile = 0).
 constexpr int kGA = 128;
-
-__device__ __forceinline__ double rsqrt_f64_adj(double x) {
-  double y0;
-  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y0) : "d"(x));
-  const double e = fma(-x, y0 * y0, 1.0);
-  return fma(y0 * e, fma(0.375, e, 0.5), y0);
-}
 
 __global__ void __launch_bounds__(kGA) k_adj_grav_f64(int n, const double4 *__restrict__ src,
                                                       const double4 *__restrict__ ab, double4 *__restrict__ xb,
-                                                      double eps2, double G) {
+                                                      double eps2, double G, int tile) {
   __shared__ double4 sp[kGA];
   __shared__ double4 sg[kGA];
   const int t = threadIdx.x;
   const int i = blockIdx.x * kGA + t;
   const int ii = min(i, n - 1);
+  const int i0 = blockIdx.x * kGA;
+  const int jlo = tile > 0 ? (i0 / tile) * tile : 0;
+  const int jhi = tile > 0 ? min(jlo + tile, n) : n;
   const double4 pi = src[ii];
   const double4 gi4 = ab[ii];
   const double mi = pi.w, gix = gi4.x, giy = gi4.y, giz = gi4.z;
   double rx = 0, ry = 0, rz = 0;
-  for (int j0 = 0; j0 < n; j0 += kGA) {
+  for (int j0 = jlo; j0 < jhi; j0 += kGA) {
     const int j = j0 + t;
     __syncthreads();
-    if (j < n) {
+    if (j < jhi) {
       sp[t] = src[j];
       const double4 g = ab[j];
       sg[t] = make_double4(g.x, g.y, g.z, 0);
@@ -217,13 +219,13 @@ __global__ void __launch_bounds__(kGA) k_adj_grav_f64(int n, const double4 *__re
       sg[t] = make_double4(0, 0, 0, 0);
     }
     __syncthreads();
-    const int m = min(kGA, n - j0);
+    const int m = min(kGA, jhi - j0);
     for (int k = 0; k < m; k++) {
       const double4 q = sp[k];
       const double4 gj = sg[k];
       const double dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
       const double s2 = fma(dz, dz, fma(dy, dy, fma(dx, dx, eps2)));
-      const double inv = rsqrt_f64_adj(s2);
+      const double inv = rsqrt_f64(s2);
       const double inv2 = inv * inv, inv3 = inv2 * inv;
       const double wx = mi * gj.x - q.w * gix, wy = mi * gj.y - q.w * giy, wz = mi * gj.z - q.w * giz;
       const double dw = dx * wx + dy * wy + dz * wz;
@@ -244,22 +246,25 @@ __global__ void __launch_bounds__(kGA) k_adj_grav_f64(int n, const double4 *__re
 // anchor, FP64 per-tile accumulation
 __global__ void __launch_bounds__(kGA) k_adj_grav_f32(int n, const double4 *__restrict__ src,
                                                       const double4 *__restrict__ ab, double4 *__restrict__ xb,
-                                                      float eps2, double G) {
+                                                      float eps2, double G, int tile) {
   __shared__ float4 sp[kGA];
   __shared__ float4 sg[kGA];
   const int t = threadIdx.x;
   const int i = blockIdx.x * kGA + t;
   const int ii = min(i, n - 1);
-  const double4 anc = src[min(blockIdx.x * kGA, n - 1)];
+  const int i0 = blockIdx.x * kGA;
+  const int jlo = tile > 0 ? (i0 / tile) * tile : 0;
+  const int jhi = tile > 0 ? min(jlo + tile, n) : n;
+  const double4 anc = src[min(i0, n - 1)];
   const double4 pi = src[ii];
   const double4 gi4 = ab[ii];
   const float xi = (float)(pi.x - anc.x), yi = (float)(pi.y - anc.y), zi = (float)(pi.z - anc.z);
   const float mi = (float)pi.w, gix = (float)gi4.x, giy = (float)gi4.y, giz = (float)gi4.z;
   double rx = 0, ry = 0, rz = 0;
-  for (int j0 = 0; j0 < n; j0 += kGA) {
+  for (int j0 = jlo; j0 < jhi; j0 += kGA) {
     const int j = j0 + t;
     __syncthreads();
-    if (j < n) {
+    if (j < jhi) {
       const double4 q = src[j];
       const double4 g = ab[j];
       sp[t] = make_float4((float)(q.x - anc.x), (float)(q.y - anc.y), (float)(q.z - anc.z), (float)q.w);
@@ -270,13 +275,13 @@ __global__ void __launch_bounds__(kGA) k_adj_grav_f32(int n, const double4 *__re
     }
     __syncthreads();
     float px = 0.f, py = 0.f, pz = 0.f;
-    const int m = min(kGA, n - j0);
+    const int m = min(kGA, jhi - j0);
     for (int k = 0; k < m; k++) {
       const float4 q = sp[k];
       const float4 gj = sg[k];
       const float dx = q.x - xi, dy = q.y - yi, dz = q.z - zi;
       const float s2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
-      const float inv = rsqrtf(s2);
+      const float inv = rsqrt_f32(s2);
       const float inv2 = inv * inv, inv3 = inv2 * inv;
       const float wx = mi * gj.x - q.w * gix, wy = mi * gj.y - q.w * giy, wz = mi * gj.z - q.w * giz;
       const float c = 3.f * inv2 * (dx * wx + dy * wy + dz * wz);
@@ -290,6 +295,224 @@ __global__ void __launch_bounds__(kGA) k_adj_grav_f32(int n, const double4 *__re
     double4 x = xb[i];
     x.x += G * rx; x.y += G * ry; x.z += G * rz;
     xb[i] = x;
+  }
+}
+
+// Symmetric mixed form: packed f32x2 i-pairs, FP32 positions relative to the
+// i-tile's FP64 anchor, sources {x, m, gbar} travelling through the lanes
+// with their FP32 j-side sums; per two pairs 31 packed FP32 instructions and
+// 2 MUFU.rsq (3 sub, 3 FMA for s^2, 3 mul for s^-2, s^-3 and -3 s^-2, 6 for
+// w, 3 for d.w, 1 for the scale, 3 FMA for w - c d, 3 mul by s^-3, 3 + 3 adds
+// into the i- and j-side sums).
+constexpr int kAdjWarps = 4;
+constexpr int kAdjRP = 4;
+constexpr int kAdjTile = kAdjWarps * 64 * kAdjRP;  // 1024
+
+__global__ void __launch_bounds__(kAdjWarps * 32) k_adj_grav_sym_f32(int n, int nt, const double4 *__restrict__ src,
+                                                                    const double4 *__restrict__ ab,
+                                                                    double4 *__restrict__ xb, float eps2, double G) {
+  __shared__ float red[2][kAdjWarps][3][32];
+  __shared__ double iacc[2 * kAdjRP * 3][kAdjWarps * 32];  // [i-slot * 3 + component][thread]
+  int b, t_lo, t_hi;
+  sym_item(blockIdx.x, nt, b, t_lo, t_hi);
+  const int j_lo = t_lo * kAdjTile, j_hi = min(t_hi * kAdjTile, n);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nxt = (l + 1) & 31;
+  const int i0 = b * kAdjTile;
+  const double4 anc = src[i0];
+  const int ib = i0 + w * 64 * kAdjRP + l;
+  f32x2 xi[kAdjRP], yi[kAdjRP], zi[kAdjRP], mi[kAdjRP], gx[kAdjRP], gy[kAdjRP], gz[kAdjRP];
+#pragma unroll
+  for (int p = 0; p < kAdjRP; p++) {
+    float x[2] = {0.f, 0.f}, y[2] = {0.f, 0.f}, z[2] = {0.f, 0.f}, m[2] = {0.f, 0.f};
+    float u[2] = {0.f, 0.f}, v[2] = {0.f, 0.f}, q[2] = {0.f, 0.f};
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int i = ib + (2 * p + h) * 32;
+      if (i < n) {  // padding i-slots: massless, no gbar, at the anchor
+        const double4 s = src[i], g = ab[i];
+        x[h] = (float)(s.x - anc.x); y[h] = (float)(s.y - anc.y); z[h] = (float)(s.z - anc.z); m[h] = (float)s.w;
+        u[h] = (float)g.x; v[h] = (float)g.y; q[h] = (float)g.z;
+      }
+#pragma unroll
+      for (int c = 0; c < 3; c++) iacc[(2 * p + h) * 3 + c][threadIdx.x] = 0.0;
+    }
+    xi[p] = pk2(x[0], x[1]); yi[p] = pk2(y[0], y[1]); zi[p] = pk2(z[0], z[1]); mi[p] = pk2(m[0], m[1]);
+    gx[p] = pk2(u[0], u[1]); gy[p] = pk2(v[0], v[1]); gz[p] = pk2(q[0], q[1]);
+  }
+  const f32x2 e2 = pk2(eps2, eps2), m3 = pk2(-3.f, -3.f);
+  int k = 0;
+  for (int jb = j_lo; jb < j_hi; jb += 32, k ^= 1) {
+    float xj = 0.f, yj = 0.f, zj = 0.f, mj = 0.f, gjx = 0.f, gjy = 0.f, gjz = 0.f;
+    if (jb + l < j_hi) {  // padding sources: massless, no gbar, at the anchor
+      const double4 s = src[jb + l], g = ab[jb + l];
+      xj = (float)(s.x - anc.x); yj = (float)(s.y - anc.y); zj = (float)(s.z - anc.z); mj = (float)s.w;
+      gjx = (float)g.x; gjy = (float)g.y; gjz = (float)g.z;
+    }
+    float ajx = 0.f, ajy = 0.f, ajz = 0.f;
+    f32x2 px[kAdjRP], py[kAdjRP], pz[kAdjRP];
+#pragma unroll
+    for (int p = 0; p < kAdjRP; p++) px[p] = py[p] = pz[p] = 0ull;
+#pragma unroll 1
+    for (int s = 0; s < 32; s++) {
+      const f32x2 XJ = pk2(xj, xj), YJ = pk2(yj, yj), ZJ = pk2(zj, zj), NMJ = pk2(-mj, -mj);
+      const f32x2 GX = pk2(gjx, gjx), GY = pk2(gjy, gjy), GZ = pk2(gjz, gjz);
+      f32x2 AX = pk2(ajx, 0.f), AY = pk2(ajy, 0.f), AZ = pk2(ajz, 0.f);
+#pragma unroll
+      for (int p = 0; p < kAdjRP; p++) {
+        const f32x2 dx = sub2(XJ, xi[p]), dy = sub2(YJ, yi[p]), dz = sub2(ZJ, zi[p]);
+        f32x2 r2 = fma2(dx, dx, e2);
+        r2 = fma2(dy, dy, r2);
+        r2 = fma2(dz, dz, r2);
+        float r2a, r2b;
+        upk2(r2, r2a, r2b);
+        const f32x2 inv = pk2(rsqrt_f32(r2a), rsqrt_f32(r2b));
+        const f32x2 inv2 = mul2(inv, inv);
+        const f32x2 inv3 = mul2(inv2, inv), nc3 = mul2(inv2, m3);
+        // w = m_i gbar_j - m_j gbar_i
+        const f32x2 wx = fma2(mi[p], GX, mul2(NMJ, gx[p]));
+        const f32x2 wy = fma2(mi[p], GY, mul2(NMJ, gy[p]));
+        const f32x2 wz = fma2(mi[p], GZ, mul2(NMJ, gz[p]));
+        const f32x2 nc = mul2(nc3, fma2(dz, wz, fma2(dy, wy, mul2(dx, wx))));  // -3 (d.w) / s^2
+        const f32x2 vx = mul2(inv3, fma2(nc, dx, wx));
+        const f32x2 vy = mul2(inv3, fma2(nc, dy, wy));
+        const f32x2 vz = mul2(inv3, fma2(nc, dz, wz));
+        px[p] = add2(px[p], vx);
+        py[p] = add2(py[p], vy);
+        pz[p] = add2(pz[p], vz);
+        AX = sub2(AX, vx);
+        AY = sub2(AY, vy);
+        AZ = sub2(AZ, vz);
+      }
+      float a0, a1;
+      upk2(AX, a0, a1); ajx = a0 + a1;
+      upk2(AY, a0, a1); ajy = a0 + a1;
+      upk2(AZ, a0, a1); ajz = a0 + a1;
+      xj = __shfl_sync(0xffffffffu, xj, nxt);
+      yj = __shfl_sync(0xffffffffu, yj, nxt);
+      zj = __shfl_sync(0xffffffffu, zj, nxt);
+      mj = __shfl_sync(0xffffffffu, mj, nxt);
+      gjx = __shfl_sync(0xffffffffu, gjx, nxt);
+      gjy = __shfl_sync(0xffffffffu, gjy, nxt);
+      gjz = __shfl_sync(0xffffffffu, gjz, nxt);
+      ajx = __shfl_sync(0xffffffffu, ajx, nxt);
+      ajy = __shfl_sync(0xffffffffu, ajy, nxt);
+      ajz = __shfl_sync(0xffffffffu, ajz, nxt);
+    }
+#pragma unroll
+    for (int p = 0; p < kAdjRP; p++) {
+      const f32x2 part[3] = {px[p], py[p], pz[p]};
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        float a0, a1;
+        upk2(part[c], a0, a1);
+        iacc[(2 * p) * 3 + c][threadIdx.x] += a0;
+        iacc[(2 * p + 1) * 3 + c][threadIdx.x] += a1;
+      }
+    }
+    red[k][w][0][l] = ajx;
+    red[k][w][1][l] = ajy;
+    red[k][w][2][l] = ajz;
+    __syncthreads();  // also orders this batch's reads of red[k] before batch + 2 writes it
+    for (int qq = threadIdx.x; qq < 96; qq += kAdjWarps * 32) {
+      const int c = qq >> 5, ll = qq & 31;
+      double sum = 0.0;
+#pragma unroll
+      for (int v = 0; v < kAdjWarps; v++) sum += (double)red[k][v][c][ll];
+      if (jb + ll < j_hi) atomicAdd(&reinterpret_cast<double *>(xb + jb + ll)[c], G * sum);
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 2 * kAdjRP; r++) {
+    const int i = ib + r * 32;
+    if (i < n) {
+      double *o = reinterpret_cast<double *>(xb + i);
+#pragma unroll
+      for (int c = 0; c < 3; c++) atomicAdd(o + c, G * iacc[r * 3 + c][threadIdx.x]);
+    }
+  }
+}
+
+// Symmetric FP64 form: absolute coordinates, kAdj64R i-particles per lane
+// with their sums in registers.
+constexpr int kAdj64Warps = 4;
+constexpr int kAdj64R = 8;
+static_assert(kAdj64Warps * 32 * kAdj64R == kAdjTile, "the FP64 form shares the tile layout");
+
+__global__ void __launch_bounds__(kAdj64Warps * 32) k_adj_grav_sym_f64(int n, int nt, const double4 *__restrict__ src,
+                                                                      const double4 *__restrict__ ab,
+                                                                      double4 *__restrict__ xb, double eps2, double G) {
+  __shared__ double red[2][kAdj64Warps][3][32];
+  int b, t_lo, t_hi;
+  sym_item(blockIdx.x, nt, b, t_lo, t_hi);
+  const int j_lo = t_lo * kAdjTile, j_hi = min(t_hi * kAdjTile, n);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nxt = (l + 1) & 31;
+  const int ib = b * kAdjTile + w * 32 * kAdj64R + l;
+  const double4 far = src[b * kAdjTile];  // position given to padding slots
+  double xi[kAdj64R], yi[kAdj64R], zi[kAdj64R], mi[kAdj64R], gx[kAdj64R], gy[kAdj64R], gz[kAdj64R];
+  double rx[kAdj64R], ry[kAdj64R], rz[kAdj64R];
+#pragma unroll
+  for (int r = 0; r < kAdj64R; r++) {
+    const int i = ib + r * 32;
+    const bool in = i < n;
+    const double4 s = in ? src[i] : make_double4(far.x, far.y, far.z, 0.0);
+    const double4 g = in ? ab[i] : make_double4(0.0, 0.0, 0.0, 0.0);
+    xi[r] = s.x; yi[r] = s.y; zi[r] = s.z; mi[r] = s.w;
+    gx[r] = g.x; gy[r] = g.y; gz[r] = g.z;
+    rx[r] = ry[r] = rz[r] = 0.0;
+  }
+  int k = 0;
+  for (int jb = j_lo; jb < j_hi; jb += 32, k ^= 1) {
+    const bool in = jb + l < j_hi;
+    const double4 s = in ? src[jb + l] : make_double4(far.x, far.y, far.z, 0.0);
+    const double4 g = in ? ab[jb + l] : make_double4(0.0, 0.0, 0.0, 0.0);
+    double xj = s.x, yj = s.y, zj = s.z, mj = s.w, gjx = g.x, gjy = g.y, gjz = g.z;
+    double ajx = 0.0, ajy = 0.0, ajz = 0.0;
+#pragma unroll 1
+    for (int st = 0; st < 32; st++) {
+#pragma unroll
+      for (int r = 0; r < kAdj64R; r++) {
+        const double dx = xj - xi[r], dy = yj - yi[r], dz = zj - zi[r];
+        const double s2 = fma(dz, dz, fma(dy, dy, fma(dx, dx, eps2)));
+        const double inv = rsqrt_f64(s2);
+        const double inv2 = inv * inv, inv3 = inv2 * inv;
+        const double wx = mi[r] * gjx - mj * gx[r], wy = mi[r] * gjy - mj * gy[r], wz = mi[r] * gjz - mj * gz[r];
+        const double c = 3.0 * inv2 * (dx * wx + dy * wy + dz * wz);
+        const double vx = inv3 * (wx - c * dx), vy = inv3 * (wy - c * dy), vz = inv3 * (wz - c * dz);
+        rx[r] += vx; ry[r] += vy; rz[r] += vz;
+        ajx -= vx; ajy -= vy; ajz -= vz;
+      }
+      xj = __shfl_sync(0xffffffffu, xj, nxt);
+      yj = __shfl_sync(0xffffffffu, yj, nxt);
+      zj = __shfl_sync(0xffffffffu, zj, nxt);
+      mj = __shfl_sync(0xffffffffu, mj, nxt);
+      gjx = __shfl_sync(0xffffffffu, gjx, nxt);
+      gjy = __shfl_sync(0xffffffffu, gjy, nxt);
+      gjz = __shfl_sync(0xffffffffu, gjz, nxt);
+      ajx = __shfl_sync(0xffffffffu, ajx, nxt);
+      ajy = __shfl_sync(0xffffffffu, ajy, nxt);
+      ajz = __shfl_sync(0xffffffffu, ajz, nxt);
+    }
+    red[k][w][0][l] = ajx;
+    red[k][w][1][l] = ajy;
+    red[k][w][2][l] = ajz;
+    __syncthreads();  // also orders this batch's reads of red[k] before batch + 2 writes it
+    for (int qq = threadIdx.x; qq < 96; qq += kAdj64Warps * 32) {
+      const int c = qq >> 5, ll = qq & 31;
+      double sum = 0.0;
+#pragma unroll
+      for (int v = 0; v < kAdj64Warps; v++) sum += red[k][v][c][ll];
+      if (jb + ll < j_hi) atomicAdd(&reinterpret_cast<double *>(xb + jb + ll)[c], G * sum);
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < kAdj64R; r++) {
+    const int i = ib + r * 32;
+    if (i < n) {
+      double *o = reinterpret_cast<double *>(xb + i);
+      atomicAdd(o + 0, G * rx[r]);
+      atomicAdd(o + 1, G * ry[r]);
+      atomicAdd(o + 2, G * rz[r]);
+    }
   }
 }
 
@@ -770,11 +993,26 @@ int launch_adjoint(AdjArgs a, const double4 *src, double eps, double G, int prec
   b.part = a.part + nb;
   k_adj_argmin<<<nb, kAT, 0, st>>>(b); launches++;
   k_adj_timestep<<<1, 32, 0, st>>>(a, nb, nb); launches++;
-  if (precision == SPH_PREC_FP64)
-    k_adj_grav_f64<<<(n + kGA - 1) / kGA, kGA, 0, st>>>(n, src, a.ab, a.xb, eps * eps, G);
-  else
-    k_adj_grav_f32<<<(n + kGA - 1) / kGA, kGA, 0, st>>>(n, src, a.ab, a.xb, (float)(eps * eps), G);
-  launches++;
+  {
+    // diagonal tiles one-sided (plain read-modify-write of xbar), then the
+    // pairs above them once each (atomics on top)
+    static_assert(kAdjTile % kGA == 0, "diagonal tiles must hold whole blocks");
+    const int nt = (n + kAdjTile - 1) / kAdjTile;
+    const int tile = nt < 2 ? 0 : kAdjTile;
+    if (precision == SPH_PREC_FP64)
+      k_adj_grav_f64<<<(n + kGA - 1) / kGA, kGA, 0, st>>>(n, src, a.ab, a.xb, eps * eps, G, tile);
+    else
+      k_adj_grav_f32<<<(n + kGA - 1) / kGA, kGA, 0, st>>>(n, src, a.ab, a.xb, (float)(eps * eps), G, tile);
+    launches++;
+    if (nt >= 2) {
+      if (precision == SPH_PREC_FP64)
+        k_adj_grav_sym_f64<<<(unsigned)sym_S(nt - 1), kAdj64Warps * 32, 0, st>>>(n, nt, src, a.ab, a.xb, eps * eps, G);
+      else
+        k_adj_grav_sym_f32<<<(unsigned)sym_S(nt - 1), kAdjWarps * 32, 0, st>>>(n, nt, src, a.ab, a.xb,
+                                                                            (float)(eps * eps), G);
+      launches++;
+    }
+  }
   k_adj_hydro<<<warps_blocks, 128, 0, st>>>(a); launches++;
   k_adj_vsig<<<1, 32, 0, st>>>(a); launches++;
   k_adj_particle<<<nb, kAT, 0, st>>>(a); launches++;

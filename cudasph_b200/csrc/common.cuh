@@ -109,6 +109,31 @@ __device__ __forceinline__ double ds2_exact(double dx, double dy, double dz) {
 
 __device__ __forceinline__ void raise_flag(unsigned *flags, unsigned f) { atomicOr(flags, f); }
 
+// Work items of the symmetric (each pair once) direct-N kernels: the Morton
+// order is cut into nt tiles; tile row b owns the nt - 1 - b tiles above the
+// diagonal, split into items of up to kSymChunk tiles, rows in order.
+constexpr int kSymChunk = 8;
+
+// S(M) = sum_{m=1..M} ceil(m / kSymChunk): items of the rows with 1..M tiles
+__host__ __device__ __forceinline__ long long sym_S(long long M) {
+  const long long q = M / kSymChunk, r = M % kSymChunk;
+  return kSymChunk * q * (q + 1) / 2 + (q + 1) * r;
+}
+// first work item of tile row b
+__host__ __device__ __forceinline__ long long sym_first(int b, int nt) { return sym_S(nt - 1) - sym_S(nt - 1 - b); }
+
+// item -> (row b, j-tiles [t_lo, t_hi)), by binary search over the rows
+__device__ __forceinline__ void sym_item(long long item, int nt, int &b, int &t_lo, int &t_hi) {
+  int lo = 0, hi = nt - 2;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (sym_first(mid, nt) <= item) lo = mid; else hi = mid - 1;
+  }
+  b = lo;
+  t_lo = b + 1 + (int)(item - sym_first(b, nt)) * kSymChunk;
+  t_hi = min(t_lo + kSymChunk, nt);
+}
+
 }  // namespace sph
 
 #define SPH_CUDA_TRY(expr)                                       \

@@ -25,24 +25,12 @@
 // (y = y0 (1 + e/2 + 3 e^2 / 8), e = 1 - r2 y0^2), checked against
 // 1/sqrt(r2) to a few ulp by the test suite.
 #include "common.cuh"
+#include "pairmath.cuh"
 
 namespace sph {
 
 constexpr int kGThreads = 128;
 
-__device__ __forceinline__ float rsqrt_f32(float x) {
-  float y;
-  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
-
-__device__ __forceinline__ double rsqrt_f64(double x) {
-  double y0;
-  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y0) : "d"(x));
-  const double e = fma(-x, y0 * y0, 1.0);
-  const double c = fma(0.375, e, 0.5);
-  return fma(y0 * e, c, y0);
-}
 
 // reference spline softening polynomials, sph_grav_kernel.cu:53-61
 template <class R>
@@ -307,31 +295,6 @@ __global__ void __launch_bounds__(kGThreads) k_grav_f32(int n, const double4 *__
 // 16-byte shared loads per thread and no repacking.  Padding sources beyond n
 // have m = 0 at the anchor; eps > 0 keeps their r^2 > 0, so every tile is a
 // full tile.
-typedef unsigned long long f32x2;
-
-__device__ __forceinline__ f32x2 pk2(float a, float b) {
-  f32x2 r;
-  asm("mov.b64 %0, {%1,%2};" : "=l"(r) : "f"(a), "f"(b));
-  return r;
-}
-__device__ __forceinline__ void upk2(f32x2 v, float &a, float &b) {
-  asm("mov.b64 {%0,%1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
-}
-__device__ __forceinline__ f32x2 sub2(f32x2 a, f32x2 b) {
-  f32x2 d;
-  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
-__device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
-  f32x2 d;
-  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
-__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
-  f32x2 d;
-  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-  return d;
-}
 
 // One-sided form: every i of the block against the sources [jlo, jhi); with
 // tile > 0 the range is the tile of `tile` particles that holds the block
@@ -455,30 +418,14 @@ __global__ void __launch_bounds__(kGThreads) k_grav_f32x2_plummer(int n, const d
 constexpr int kSymWarps = 2;
 constexpr int kSymRP = 8;
 constexpr int kSymTile = kSymWarps * 64 * kSymRP;  // 1024 i-particles per block
-constexpr int kSymChunk = 8;                        // j-tiles per work item
-
-// S(M) = sum_{m=1..M} ceil(m / kSymChunk): items of the rows with 1..M tiles
-__host__ __device__ __forceinline__ long long sym_S(long long M) {
-  const long long q = M / kSymChunk, r = M % kSymChunk;
-  return kSymChunk * q * (q + 1) / 2 + (q + 1) * r;
-}
-// first work item of tile row b (row b has nt - 1 - b tiles above the diagonal)
-__host__ __device__ __forceinline__ long long sym_first(int b, int nt) { return sym_S(nt - 1) - sym_S(nt - 1 - b); }
 
 __global__ void __launch_bounds__(kSymWarps * 32, 4) k_grav_sym_plummer(int n, int nt, const double4 *__restrict__ src,
                                                                          double4 *__restrict__ out, float eps2,
                                                                          double G) {
   __shared__ float red[2][kSymWarps][4][32];
   __shared__ double iacc[2 * kSymRP * 4][kSymWarps * 32];  // [i-slot * 4 + component][thread]
-  const long long item = blockIdx.x;
-  int lo = 0, hi = nt - 2;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (sym_first(mid, nt) <= item) lo = mid; else hi = mid - 1;
-  }
-  const int b = lo;
-  const int t_lo = b + 1 + (int)(item - sym_first(b, nt)) * kSymChunk;
-  const int t_hi = min(t_lo + kSymChunk, nt);
+  int b, t_lo, t_hi;
+  sym_item(blockIdx.x, nt, b, t_lo, t_hi);
   const int j_lo = t_lo * kSymTile, j_hi = min(t_hi * kSymTile, n);
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nxt = (l + 1) & 31;
   const int i0 = b * kSymTile;
@@ -602,15 +549,8 @@ static_assert(kSym64Warps * 32 * kSym64R == kSymTile, "the FP64 form shares the 
 __global__ void __launch_bounds__(kSym64Warps * 32) k_grav_sym_f64(int n, int nt, const double4 *__restrict__ src,
                                                                   double4 *__restrict__ out, double eps2, double G) {
   __shared__ double red[2][kSym64Warps][4][32];
-  const long long item = blockIdx.x;
-  int lo = 0, hi = nt - 2;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (sym_first(mid, nt) <= item) lo = mid; else hi = mid - 1;
-  }
-  const int b = lo;
-  const int t_lo = b + 1 + (int)(item - sym_first(b, nt)) * kSymChunk;
-  const int t_hi = min(t_lo + kSymChunk, nt);
+  int b, t_lo, t_hi;
+  sym_item(blockIdx.x, nt, b, t_lo, t_hi);
   const int j_lo = t_lo * kSymTile, j_hi = min(t_hi * kSymTile, n);
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nxt = (l + 1) & 31;
   const int ib = b * kSymTile + w * 32 * kSym64R + l;
