@@ -170,17 +170,60 @@ def traffic_from_profiles(kernel_tag: str, n: int):
     return b0 * (n / n0)
 
 
+def measured_hbm_gbs():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (measured copy bandwidth)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback 6.65 TB/s (no measured peaks file)"
+
+
+# Algorithmic bytes per particle of the bandwidth-bound phases, each stream
+# counted once; nbar = mean neighbour count.  Neighbour records gathered by the
+# list loops (64-128 B per pair) are Morton-close and served by L1/L2; they
+# are not part of the algorithmic figure.
+SPH_BYTES = {
+    # pos read 32; range 8, count 4 and the list 4 nbar written
+    "solve_range": lambda nb: 32 + 8 + 4 + 4 * nb,
+    # list 4 nbar + count 4 + own pos/vel 64 read; rho 8 + div/curl/omega/psi 32 written
+    "density": lambda nb: 4 * nb + 4 + 64 + 40,
+    # rho, P, u, mu 32 read; P 8 written
+    "pressure": lambda nb: 40,
+    # list 4 nbar + count 4 + own pos/vel/hyd/dd 128 read; dots 32 + vsig 8 written
+    "hydro": lambda nb: 4 * nb + 4 + 128 + 40,
+    # bounding box 32 + Morton keys (32 read, 12 written) + 8 radix passes x (12 read + 12 written)
+    # + permutation of the state (204 read + 204 written + 4 index)
+    "sort": lambda nb: 32 + 44 + 8 * 24 + 412,
+}
+
+
+def sph_bandwidth(ph, steps, n, nbar):
+    """Achieved HBM bandwidth of the bandwidth-bound phases (device time per
+    step from the CUDA-event phase timers) against the measured copy peak."""
+    peak, src = measured_hbm_gbs()
+    out = {"peak_gbs": peak, "peak_source": src, "mean_neighbours": nbar}
+    for k, f in SPH_BYTES.items():
+        if k not in ph or ph[k][0] <= 0:
+            continue
+        ms = ph[k][0] / steps
+        b = f(nbar) * n
+        out[k] = {"ms": round(ms, 4), "bytes_per_particle": round(f(nbar), 1), "gbs": round(b / (ms * 1e-3) / 1e9, 1),
+                  "frac": round(b / (ms * 1e-3) / 1e9 / peak, 4)}
+    return out
+
+
 ADJOINT_N = 65536
 ADJOINT_PARAMS = dict(n_target=50.0, eos_mode=1, soft_mode=1, eps=0.01)
 
 
-def adjoint_cost(steps=3, warmup=3, headline_n=None):
+def adjoint_cost(steps=5, warmup=3, headline_n=None):
     """Cost of the hand-written adjoint of one step relative to the forward
     step, on the differentiation workload: an n=3 polytrope, N = 65,536,
     ideal gas + radiation EOS, N_ngb = 50, Plummer eps = 0.01.  Device time
     (CUDA events) of the forward step taken with keep on vs the reverse sweep
-    (cudasph_adjoint) of the same step; a checkpointed rollout additionally
-    replays each step once before its reverse sweep."""
+    (cudasph_adjoint) of the same step, each the median over `steps`
+    step + adjoint iterations; a checkpointed rollout additionally replays
+    each step once before its reverse sweep."""
     from cudasph_b200 import ics
     from cudasph_b200.simulation import Simulation, make_params
     ic = ics.polytrope(ADJOINT_N, n_poly=3.0, n_ngb=50.0, seed=12345 + 4, mu=0.62)
@@ -197,20 +240,21 @@ def adjoint_cost(steps=3, warmup=3, headline_n=None):
         m = ic["m"]
         for _ in range(warmup):  # warm-up includes the reverse sweep (first use of its kernels)
             step_and_adjoint(sim, m)
-        sim.synchronize()
-        sim.reset_counters()
-        sim.set_profiling(True)
+        fwd_s, adj_s = [], []
         for _ in range(steps):
-            sim.step()
-            for k, v in (("vx", m * sim.get("vx")), ("vy", m * sim.get("vy")), ("vz", m * sim.get("vz"))):
-                sim.adjoint_set(k, v)
-            sim.adjoint()
-        ph = sim.phase_times()
-        sim.set_profiling(False)
-        fwd = sum(v[0] for k, v in ph.items() if k != "adjoint") / steps
-        adj = ph["adjoint"][0] / steps
+            sim.synchronize()
+            sim.reset_counters()
+            sim.set_profiling(True)
+            step_and_adjoint(sim, m)
+            ph = sim.phase_times()
+            sim.set_profiling(False)
+            fwd_s.append(sum(v[0] for k, v in ph.items() if k != "adjoint"))
+            adj_s.append(ph["adjoint"][0])
+        fwd, adj = float(np.median(fwd_s)), float(np.median(adj_s))
         out[name] = {"forward_ms": fwd, "adjoint_ms": adj, "adjoint_over_forward": adj / fwd,
-                     "replay_plus_adjoint_over_forward": (fwd + adj) / fwd, "flags": sim.device_status()}
+                     "replay_plus_adjoint_over_forward": (fwd + adj) / fwd, "flags": sim.device_status(),
+                     "samples_forward_ms": [round(v, 3) for v in fwd_s],
+                     "samples_adjoint_ms": [round(v, 3) for v in adj_s]}
         sim.close()
     if headline_n:
         # the same ratio on the headline workload (mixed form, one step)
@@ -425,6 +469,7 @@ def run_ours(args, rank, world):
                        "flops_per_launch": flops, "launch_ms": grav_ms,
                        "interactions_per_s": n * n / (grav_ms * 1e-3)}
     out["stats_last_step"] = {k: stats[k] for k in ("E", "W", "T", "U", "dt", "ngb_mean", "ngb_min", "ngb_max")}
+    out["sph_roofline"] = sph_bandwidth(ph, args.steps, n, stats["ngb_mean"])
 
     # --- FP64 comparison and errors ----------------------------------------------
     if not args.fp64_only and args.fp64_steps > 0:

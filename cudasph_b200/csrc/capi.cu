@@ -29,8 +29,9 @@ int launch_hydro(const HydroArgs &a, cudaStream_t st);
 int launch_density_mixed(const HydroArgs &a, cudaStream_t st);
 int launch_hydro_mixed(const HydroArgs &a, cudaStream_t st);
 int launch_gravity(int n, const double4 *src, const double *h2src, double4 *out, int soft_mode, double eps, double G,
-                   int precision, cudaStream_t st);
-int launch_pack_sources(int n, const double4 *pos, const double4 *vel, double4 *src, double *h2, cudaStream_t st);
+                   int precision, const int *mass_mixed, cudaStream_t st);
+int launch_pack_sources(int n, const double4 *pos, const double4 *vel, double4 *src, double *h2, int *mass_mixed,
+                        cudaStream_t st);
 int launch_predict(int n, double4 *pos, double4 *vel, double4 *hyd, const double4 *dots, double4 *old,
                    const double *sc, cudaStream_t st);
 int finish_partial_doubles(int n);
@@ -82,6 +83,7 @@ struct sph_ctx {
   double *bbox_part = nullptr, *box4 = nullptr;
   double4 *gsrc = nullptr;
   double *gh2 = nullptr;
+  int *mass_mixed = nullptr;  // 0 when all masses are equal (set with the gravity sources)
   unsigned *flags = nullptr;
   double *sc = nullptr;  // StepScalars
   double *fin_part = nullptr;
@@ -249,7 +251,7 @@ extern "C" int cudasph_destroy(sph_ctx *c) {
   }
   cudaFree(c->old); cudaFree(c->n_ngb); cudaFree(c->nevals); cudaFree(c->list); cudaFree(c->dcache);
   cudaFree(c->tlo); cudaFree(c->thi); cudaFree(c->keys); cudaFree(c->vals); cudaFree(c->sort_scratch);
-  cudaFree(c->bbox_part); cudaFree(c->box4); cudaFree(c->gsrc); cudaFree(c->gh2); cudaFree(c->flags);
+  cudaFree(c->bbox_part); cudaFree(c->box4); cudaFree(c->gsrc); cudaFree(c->gh2); cudaFree(c->mass_mixed); cudaFree(c->flags);
   cudaFree(c->sc); cudaFree(c->fin_part); cudaFree(c->flat); cudaFree(c->slot_of);
   cudaFree(c->pre_acc); cudaFree(c->xb); cudaFree(c->vb); cudaFree(c->ab); cudaFree(c->vpb); cudaFree(c->vpup);
   cudaFree(c->rhob); cudaFree(c->Pb); cudaFree(c->omb); cudaFree(c->psib); cudaFree(c->divb); cudaFree(c->curlb);
@@ -310,6 +312,7 @@ extern "C" int cudasph_create(const sph_params *params, int n, int device, sph_c
   TRY_ALLOC(dalloc(&c->box4, 4));
   TRY_ALLOC(dalloc(&c->gsrc, n));
   TRY_ALLOC(dalloc(&c->gh2, n));
+  TRY_ALLOC(dalloc(&c->mass_mixed, 1));
   TRY_ALLOC(dalloc(&c->flags, 1));
   TRY_ALLOC(dalloc(&c->sc, 4 + SPH_NSTATS));
   TRY_ALLOC(dalloc(&c->fin_part, finish_partial_doubles(n)));
@@ -632,8 +635,9 @@ extern "C" int cudasph_gravity(sph_ctx *c) {
   SPH_CUDA_TRY(cudaSetDevice(c->device));
   PhaseScope ps(c, SPH_PH_GRAVITY);
   Fields &F = c->f[c->cur];
-  LAUNCHED(launch_pack_sources(c->n, F.pos, F.vel, c->gsrc, c->gh2, c->st));
-  LAUNCHED(launch_gravity(c->n, c->gsrc, c->gh2, F.grav, c->p.soft_mode, c->p.eps, c->p.G, c->p.precision, c->st));
+  LAUNCHED(launch_pack_sources(c->n, F.pos, F.vel, c->gsrc, c->gh2, c->mass_mixed, c->st));
+  LAUNCHED(launch_gravity(c->n, c->gsrc, c->gh2, F.grav, c->p.soft_mode, c->p.eps, c->p.G, c->p.precision,
+                          c->mass_mixed, c->st));
   SPH_CUDA_TRY(cudaGetLastError());
   return SPH_OK;
 }

@@ -415,15 +415,23 @@ __global__ void __launch_bounds__(kGThreads) k_grav_f32x2_plummer(int n, const d
 // The output therefore holds the diagonal-tile sums first (stored by the
 // one-sided kernel) and receives the off-diagonal sums by atomics, so the
 // order of the FP64 additions, not their values, varies between runs.
+//
+// Equal masses (UNI): when every particle has the same mass m (a flag the
+// source-packing kernel computes on the device every step), the mass factors
+// out of both sums -- a_i = m sum_j d / s^3, a_j = -m sum_i d / s^3,
+// phi = -m sum 1/s -- and is applied once per batch partial (FP64) instead
+// of per pair: 16 packed instructions per two pairs instead of 18, the same
+// interactions.  Padding sources of a ragged last j-tile sit 1e18 away (their
+// d / s^3 underflows to 0) and carry potential weight 0.
 constexpr int kSymWarps = 2;
 constexpr int kSymRP = 8;
 constexpr int kSymTile = kSymWarps * 64 * kSymRP;  // 1024 i-particles per block
 
-__global__ void __launch_bounds__(kSymWarps * 32, 4) k_grav_sym_plummer(int n, int nt, const double4 *__restrict__ src,
-                                                                         double4 *__restrict__ out, float eps2,
-                                                                         double G) {
-  __shared__ float red[2][kSymWarps][4][32];
-  __shared__ double iacc[2 * kSymRP * 4][kSymWarps * 32];  // [i-slot * 4 + component][thread]
+template <bool UNI>
+__device__ __forceinline__ void sym_plummer_item(int n, int nt, const double4 *__restrict__ src,
+                                                 double4 *__restrict__ out, float eps2, double G,
+                                                 float (&red)[2][kSymWarps][4][32],
+                                                 double (&iacc)[2 * kSymRP * 4][kSymWarps * 32]) {
   int b, t_lo, t_hi;
   sym_item(blockIdx.x, nt, b, t_lo, t_hi);
   const int j_lo = t_lo * kSymTile, j_hi = min(t_hi * kSymTile, n);
@@ -431,6 +439,8 @@ __global__ void __launch_bounds__(kSymWarps * 32, 4) k_grav_sym_plummer(int n, i
   const int i0 = b * kSymTile;
   const double4 anc = src[i0];
   const int ib = i0 + w * 64 * kSymRP + l;
+  // UNI: the common mass, applied to the i-side (+m) and j-side (-m) partials
+  const double mi_scale = UNI ? src[0].w : 1.0, mj_scale = UNI ? -src[0].w : 1.0;
 
   f32x2 xi[kSymRP], yi[kSymRP], zi[kSymRP], nmi[kSymRP];
 #pragma unroll
@@ -438,7 +448,7 @@ __global__ void __launch_bounds__(kSymWarps * 32, 4) k_grav_sym_plummer(int n, i
     float x[2] = {0.f, 0.f}, y[2] = {0.f, 0.f}, z[2] = {0.f, 0.f}, m[2] = {0.f, 0.f};
 #pragma unroll
     for (int h = 0; h < 2; h++) {
-      const int i = ib + (2 * p + h) * 32;
+      const int i = ib + (2 * p + h) * 32;  // i-tiles of work items are full tiles (b < nt - 1)
       if (i < n) {
         const double4 q = src[i];
         x[h] = (float)(q.x - anc.x); y[h] = (float)(q.y - anc.y); z[h] = (float)(q.z - anc.z); m[h] = -(float)q.w;
@@ -451,10 +461,11 @@ __global__ void __launch_bounds__(kSymWarps * 32, 4) k_grav_sym_plummer(int n, i
   const f32x2 e2 = pk2(eps2, eps2);
   int k = 0;
   for (int jb = j_lo; jb < j_hi; jb += 32, k ^= 1) {
-    float xj = 0.f, yj = 0.f, zj = 0.f, mj = 0.f;  // padding source: at the anchor, massless
+    // padding source: massless at the anchor; UNI: far away with potential weight 0
+    float xj = UNI ? 1e18f : 0.f, yj = xj, zj = xj, mj = 0.f;
     if (jb + l < j_hi) {
       const double4 q = src[jb + l];
-      xj = (float)(q.x - anc.x); yj = (float)(q.y - anc.y); zj = (float)(q.z - anc.z); mj = (float)q.w;
+      xj = (float)(q.x - anc.x); yj = (float)(q.y - anc.y); zj = (float)(q.z - anc.z); mj = UNI ? 1.f : (float)q.w;
     }
     float ajx = 0.f, ajy = 0.f, ajz = 0.f, ajp = 0.f;
     f32x2 px[kSymRP], py[kSymRP], pz[kSymRP], pp[kSymRP];
@@ -474,15 +485,26 @@ __global__ void __launch_bounds__(kSymWarps * 32, 4) k_grav_sym_plummer(int n, i
         upk2(r2, r2a, r2b);
         const f32x2 inv = pk2(rsqrt_f32(r2a), rsqrt_f32(r2b));
         const f32x2 inv3 = mul2(mul2(inv, inv), inv);
-        const f32x2 sj = mul2(MJ, inv3), si = mul2(nmi[p], inv3);  // m_j / s^3, -m_i / s^3
-        px[p] = fma2(dx, sj, px[p]);
-        py[p] = fma2(dy, sj, py[p]);
-        pz[p] = fma2(dz, sj, pz[p]);
-        pp[p] = fma2(MJ, inv, pp[p]);
-        AX = fma2(dx, si, AX);
-        AY = fma2(dy, si, AY);
-        AZ = fma2(dz, si, AZ);
-        AP = fma2(nmi[p], inv, AP);
+        if (UNI) {  // MJ = potential weight (1, or 0 for padding)
+          px[p] = fma2(dx, inv3, px[p]);
+          py[p] = fma2(dy, inv3, py[p]);
+          pz[p] = fma2(dz, inv3, pz[p]);
+          pp[p] = fma2(MJ, inv, pp[p]);
+          AX = fma2(dx, inv3, AX);
+          AY = fma2(dy, inv3, AY);
+          AZ = fma2(dz, inv3, AZ);
+          AP = add2(AP, inv);
+        } else {
+          const f32x2 sj = mul2(MJ, inv3), si = mul2(nmi[p], inv3);  // m_j / s^3, -m_i / s^3
+          px[p] = fma2(dx, sj, px[p]);
+          py[p] = fma2(dy, sj, py[p]);
+          pz[p] = fma2(dz, sj, pz[p]);
+          pp[p] = fma2(MJ, inv, pp[p]);
+          AX = fma2(dx, si, AX);
+          AY = fma2(dy, si, AY);
+          AZ = fma2(dz, si, AZ);
+          AP = fma2(nmi[p], inv, AP);
+        }
       }
       float a0, a1;
       upk2(AX, a0, a1); ajx = a0 + a1;
@@ -505,7 +527,7 @@ __global__ void __launch_bounds__(kSymWarps * 32, 4) k_grav_sym_plummer(int n, i
       for (int c = 0; c < 4; c++) {
         float a0, a1;
         upk2(part[c], a0, a1);
-        if (c == 3) a0 = -a0, a1 = -a1;  // pp holds +m/r
+        if (c == 3) a0 = -a0, a1 = -a1;  // pp holds +m/r (UNI: +1/r)
         iacc[(2 * p) * 4 + c][threadIdx.x] += a0;
         iacc[(2 * p + 1) * 4 + c][threadIdx.x] += a1;
       }
@@ -520,7 +542,7 @@ __global__ void __launch_bounds__(kSymWarps * 32, 4) k_grav_sym_plummer(int n, i
       double s = 0.0;
 #pragma unroll
       for (int v = 0; v < kSymWarps; v++) s += (double)red[k][v][c][ll];
-      if (jb + ll < j_hi) atomicAdd(&reinterpret_cast<double *>(out + jb + ll)[c], G * s);
+      if (jb + ll < j_hi) atomicAdd(&reinterpret_cast<double *>(out + jb + ll)[c], G * mj_scale * s);
     }
   }
 #pragma unroll
@@ -529,9 +551,21 @@ __global__ void __launch_bounds__(kSymWarps * 32, 4) k_grav_sym_plummer(int n, i
     if (i < n) {
       double *o = reinterpret_cast<double *>(out + i);
 #pragma unroll
-      for (int c = 0; c < 4; c++) atomicAdd(o + c, G * iacc[r * 4 + c][threadIdx.x]);
+      for (int c = 0; c < 4; c++) atomicAdd(o + c, G * mi_scale * iacc[r * 4 + c][threadIdx.x]);
     }
   }
+}
+
+// mass_mixed: device word, 0 when all masses are equal (nullptr: general form)
+__global__ void __launch_bounds__(kSymWarps * 32, 4) k_grav_sym_plummer(int n, int nt, const double4 *__restrict__ src,
+                                                                         double4 *__restrict__ out, float eps2,
+                                                                         double G, const int *__restrict__ mass_mixed) {
+  __shared__ float red[2][kSymWarps][4][32];
+  __shared__ double iacc[2 * kSymRP * 4][kSymWarps * 32];  // [i-slot * 4 + component][thread]
+  if (mass_mixed != nullptr && __ldg(mass_mixed) == 0)
+    sym_plummer_item<true>(n, nt, src, out, eps2, G, red, iacc);
+  else
+    sym_plummer_item<false>(n, nt, src, out, eps2, G, red, iacc);
 }
 
 // ------------------- FP64, symmetric pair form ------------------------------
@@ -541,35 +575,41 @@ __global__ void __launch_bounds__(kSymWarps * 32, 4) k_grav_sym_plummer(int n, i
 // FP64 sums in registers for the whole item.  Per pair: 3 sub, 3 FMA for
 // s^2, the FP64 rsqrt (MUFU seed + one Householder step: 5 FP64 ops),
 // 2 mul for s^-3, 2 for the mass-weighted s^-3 of each side, 8 FMA into the
-// i- and j-side sums -- 23 FP64 operations against 36 for both directions.
+// i- and j-side sums -- 23 FP64 operations against 36 for both directions;
+// 21 in the equal-mass form (the mass applied to the sums at the end, as in
+// the mixed kernel; padding sources 1e150 away with potential weight 0).
 constexpr int kSym64Warps = 4;
 constexpr int kSym64R = 8;
 static_assert(kSym64Warps * 32 * kSym64R == kSymTile, "the FP64 form shares the tile layout");
 
-__global__ void __launch_bounds__(kSym64Warps * 32) k_grav_sym_f64(int n, int nt, const double4 *__restrict__ src,
-                                                                  double4 *__restrict__ out, double eps2, double G) {
-  __shared__ double red[2][kSym64Warps][4][32];
+template <bool UNI>
+__device__ __forceinline__ void sym_f64_item(int n, int nt, const double4 *__restrict__ src, double4 *__restrict__ out,
+                                             double eps2, double G, double (&red)[2][kSym64Warps][4][32]) {
   int b, t_lo, t_hi;
   sym_item(blockIdx.x, nt, b, t_lo, t_hi);
   const int j_lo = t_lo * kSymTile, j_hi = min(t_hi * kSymTile, n);
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nxt = (l + 1) & 31;
   const int ib = b * kSymTile + w * 32 * kSym64R + l;
   const double4 far = src[b * kSymTile];  // position given to padding i-slots
+  const double mi_scale = UNI ? src[0].w : 1.0, mj_scale = UNI ? -src[0].w : 1.0;
 
   double xi[kSym64R], yi[kSym64R], zi[kSym64R], nmi[kSym64R];
   double ax[kSym64R], ay[kSym64R], az[kSym64R], ap[kSym64R];
 #pragma unroll
   for (int r = 0; r < kSym64R; r++) {
-    const int i = ib + r * 32;
+    const int i = ib + r * 32;  // i-tiles of work items are full tiles (b < nt - 1)
     const double4 q = i < n ? src[i] : make_double4(far.x, far.y, far.z, 0.0);
     xi[r] = q.x; yi[r] = q.y; zi[r] = q.z; nmi[r] = -q.w;
     ax[r] = ay[r] = az[r] = ap[r] = 0.0;
   }
   int k = 0;
   for (int jb = j_lo; jb < j_hi; jb += 32, k ^= 1) {
-    // padding source: massless, at a real position of the i-tile (s^2 >= eps^2 > 0)
-    const double4 q = (jb + l < j_hi) ? src[jb + l] : make_double4(far.x, far.y, far.z, 0.0);
-    double xj = q.x, yj = q.y, zj = q.z, mj = q.w;
+    // padding source: massless at a real position of the i-tile (s^2 >= eps^2 > 0);
+    // UNI: 1e150 away (d / s^3 underflows to 0) with potential weight 0
+    const bool real = jb + l < j_hi;
+    const double4 q = real ? src[jb + l] : (UNI ? make_double4(1e150, 1e150, 1e150, 0.0)
+                                                : make_double4(far.x, far.y, far.z, 0.0));
+    double xj = q.x, yj = q.y, zj = q.z, mj = UNI ? (real ? 1.0 : 0.0) : q.w;
     double bx = 0.0, by = 0.0, bz = 0.0, bp = 0.0;
 #pragma unroll 1
     for (int s = 0; s < 32; s++) {
@@ -579,15 +619,26 @@ __global__ void __launch_bounds__(kSym64Warps * 32) k_grav_sym_f64(int n, int nt
         const double r2 = fma(dz, dz, fma(dy, dy, fma(dx, dx, eps2)));
         const double inv = rsqrt_f64(r2);
         const double inv3 = inv * inv * inv;
-        const double sj = mj * inv3, si = nmi[r] * inv3;  // m_j / s^3, -m_i / s^3
-        ax[r] = fma(dx, sj, ax[r]);
-        ay[r] = fma(dy, sj, ay[r]);
-        az[r] = fma(dz, sj, az[r]);
-        ap[r] = fma(-mj, inv, ap[r]);
-        bx = fma(dx, si, bx);
-        by = fma(dy, si, by);
-        bz = fma(dz, si, bz);
-        bp = fma(nmi[r], inv, bp);
+        if (UNI) {  // mj = potential weight (1, or 0 for padding)
+          ax[r] = fma(dx, inv3, ax[r]);
+          ay[r] = fma(dy, inv3, ay[r]);
+          az[r] = fma(dz, inv3, az[r]);
+          ap[r] = fma(-mj, inv, ap[r]);
+          bx = fma(dx, inv3, bx);
+          by = fma(dy, inv3, by);
+          bz = fma(dz, inv3, bz);
+          bp += inv;
+        } else {
+          const double sj = mj * inv3, si = nmi[r] * inv3;  // m_j / s^3, -m_i / s^3
+          ax[r] = fma(dx, sj, ax[r]);
+          ay[r] = fma(dy, sj, ay[r]);
+          az[r] = fma(dz, sj, az[r]);
+          ap[r] = fma(-mj, inv, ap[r]);
+          bx = fma(dx, si, bx);
+          by = fma(dy, si, by);
+          bz = fma(dz, si, bz);
+          bp = fma(nmi[r], inv, bp);
+        }
       }
       xj = __shfl_sync(0xffffffffu, xj, nxt);
       yj = __shfl_sync(0xffffffffu, yj, nxt);
@@ -608,7 +659,7 @@ __global__ void __launch_bounds__(kSym64Warps * 32) k_grav_sym_f64(int n, int nt
       double sum = 0.0;
 #pragma unroll
       for (int v = 0; v < kSym64Warps; v++) sum += red[k][v][c][ll];
-      if (jb + ll < j_hi) atomicAdd(&reinterpret_cast<double *>(out + jb + ll)[c], G * sum);
+      if (jb + ll < j_hi) atomicAdd(&reinterpret_cast<double *>(out + jb + ll)[c], G * mj_scale * sum);
     }
   }
 #pragma unroll
@@ -616,17 +667,27 @@ __global__ void __launch_bounds__(kSym64Warps * 32) k_grav_sym_f64(int n, int nt
     const int i = ib + r * 32;
     if (i < n) {
       double *o = reinterpret_cast<double *>(out + i);
-      atomicAdd(o + 0, G * ax[r]);
-      atomicAdd(o + 1, G * ay[r]);
-      atomicAdd(o + 2, G * az[r]);
-      atomicAdd(o + 3, G * ap[r]);
+      atomicAdd(o + 0, G * mi_scale * ax[r]);
+      atomicAdd(o + 1, G * mi_scale * ay[r]);
+      atomicAdd(o + 2, G * mi_scale * az[r]);
+      atomicAdd(o + 3, G * mi_scale * ap[r]);
     }
   }
 }
 
+__global__ void __launch_bounds__(kSym64Warps * 32) k_grav_sym_f64(int n, int nt, const double4 *__restrict__ src,
+                                                                  double4 *__restrict__ out, double eps2, double G,
+                                                                  const int *__restrict__ mass_mixed) {
+  __shared__ double red[2][kSym64Warps][4][32];
+  if (mass_mixed != nullptr && __ldg(mass_mixed) == 0)
+    sym_f64_item<true>(n, nt, src, out, eps2, G, red);
+  else
+    sym_f64_item<false>(n, nt, src, out, eps2, G, red);
+}
+
 // src = {x, y, z, m} per particle; h2src = range^2 (spline mode only)
 int launch_gravity(int n, const double4 *src, const double *h2src, double4 *out, int soft_mode, double eps, double G,
-                   int precision, cudaStream_t st) {
+                   int precision, const int *mass_mixed, cudaStream_t st) {
   if (n <= 0) return 0;
   const double eps2 = eps * eps;
   if (precision == SPH_PREC_FP64) {
@@ -639,7 +700,8 @@ int launch_gravity(int n, const double4 *src, const double *h2src, double4 *out,
         k_grav_f64<SPH_SOFT_PLUMMER, R><<<blocks, kGThreads, 0, st>>>(n, src, h2src, out, eps2, G, 0);
       } else {
         k_grav_f64<SPH_SOFT_PLUMMER, R><<<blocks, kGThreads, 0, st>>>(n, src, h2src, out, eps2, G, kSymTile);
-        k_grav_sym_f64<<<(unsigned)sym_S(nt - 1), kSym64Warps * 32, 0, st>>>(n, nt, src, out, eps2, G);
+        k_grav_sym_f64<<<(unsigned)sym_S(nt - 1), kSym64Warps * 32, 0, st>>>(n, nt, src, out, eps2, G,
+                                                                              mass_mixed);
       }
     } else {
       k_grav_f64<SPH_SOFT_SPLINE, R><<<blocks, kGThreads, 0, st>>>(n, src, h2src, out, eps2, G, 0);
@@ -658,7 +720,8 @@ int launch_gravity(int n, const double4 *src, const double *h2src, double4 *out,
         // diagonal tiles store, the symmetric items add on top
         k_grav_f32x2_plummer<RP><<<blocks, kGThreads, 0, st>>>(n, src, out, (float)eps2, G, kSymTile);
         const long long items = sym_S(nt - 1);
-        k_grav_sym_plummer<<<(unsigned)items, kSymWarps * 32, 0, st>>>(n, nt, src, out, (float)eps2, G);
+        k_grav_sym_plummer<<<(unsigned)items, kSymWarps * 32, 0, st>>>(n, nt, src, out, (float)eps2, G,
+                                                                         mass_mixed);
       }
     } else {
       constexpr int R = 4;
@@ -670,17 +733,27 @@ int launch_gravity(int n, const double4 *src, const double *h2src, double4 *out,
 }
 
 // pack the gravity sources {x, y, z, m} and range^2 from the state
+// Also raises *mass_mixed (cleared before the launch) when some mass differs
+// from the first particle's: the symmetric kernels take their equal-mass form
+// when it stays 0.
 __global__ void k_pack_sources(int n, const double4 *__restrict__ pos, const double4 *__restrict__ vel,
-                               double4 *__restrict__ src, double *__restrict__ h2) {
+                               double4 *__restrict__ src, double *__restrict__ h2, int *__restrict__ mass_mixed) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const double4 p = pos[i];
-  src[i] = make_double4(p.x, p.y, p.z, vel[i].w);
-  h2[i] = p.w * p.w;
+  bool differs = false;
+  if (i < n) {
+    const double4 p = pos[i];
+    const double m = vel[i].w;
+    src[i] = make_double4(p.x, p.y, p.z, m);
+    h2[i] = p.w * p.w;
+    differs = m != __ldg(&vel[0].w);
+  }
+  if (__syncthreads_or(differs) && threadIdx.x == 0) atomicOr(mass_mixed, 1);
 }
 
-int launch_pack_sources(int n, const double4 *pos, const double4 *vel, double4 *src, double *h2, cudaStream_t st) {
-  k_pack_sources<<<(n + 255) / 256, 256, 0, st>>>(n, pos, vel, src, h2);
+int launch_pack_sources(int n, const double4 *pos, const double4 *vel, double4 *src, double *h2, int *mass_mixed,
+                        cudaStream_t st) {
+  cudaMemsetAsync(mass_mixed, 0, sizeof(int), st);
+  k_pack_sources<<<(n + 255) / 256, 256, 0, st>>>(n, pos, vel, src, h2, mass_mixed);
   return 1;
 }
 
@@ -703,7 +776,7 @@ extern "C" int cudasph_gravity_direct(int n, const double *pos4, const double *r
     SPH_CUDA_TRY(cudaMallocAsync((void **)&h2, sizeof(double) * n, st));
     sph::k_range_sq<<<(n + 255) / 256, 256, 0, st>>>(n, range, h2);
   }
-  sph::launch_gravity(n, (const double4 *)pos4, h2, (double4 *)out4, soft_mode, eps, G, precision, st);
+  sph::launch_gravity(n, (const double4 *)pos4, h2, (double4 *)out4, soft_mode, eps, G, precision, nullptr, st);
   if (h2) SPH_CUDA_TRY(cudaFreeAsync(h2, st));
   SPH_CUDA_TRY(cudaGetLastError());
   return SPH_OK;

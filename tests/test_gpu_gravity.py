@@ -80,3 +80,40 @@ def test_mixed_pair_forces_conserve_momentum():
     got = _run(p, m, 0.004, 1.0, 1)
     ma = got[:, :3] * m[:, None]
     assert np.linalg.norm(ma.sum(0)) < 1e-6 * np.abs(ma).sum()
+
+
+# The step's gravity phase takes the equal-mass form of the symmetric kernels
+# (the mass factored out of both pair sums) when every mass equals the first,
+# a flag computed on the device with the gravity sources; otherwise the
+# general form.  Both must agree with the standalone entry point, which always
+# runs the general form, and with the oracle.  n = 5000 gives five 1,024-tiles
+# (symmetric items plus a ragged last tile whose padding sources the
+# equal-mass form parks far away).
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("equal", [True, False])
+def test_step_gravity_equal_mass_form(precision, equal):
+    from cudasph_b200 import ics
+    from cudasph_b200.simulation import Simulation, make_params
+    ic = ics.polytrope(5000, n_ngb=50, seed=21)
+    if not equal:
+        ic["m"] = ic["m"] * np.random.default_rng(2).uniform(0.5, 1.5, ic["m"].size)
+    eps, G = 0.004, 1.3
+    sim = Simulation(ic, make_params(precision=precision, n_target=50.0, soft_mode=1, eps=eps, G=G))
+    sim.CUDA_gravity()
+    got = np.stack([sim.get(k) for k in ("gx", "gy", "gz", "phi")], 1)
+    order = sim.order()  # the step computes in its own (input or tree) order
+    sim.close()
+    p = np.stack([ic["x"], ic["y"], ic["z"]], 1)
+    gen = np.empty_like(got)
+    gen[order] = _run(p[order], ic["m"][order], eps, G, precision)
+    ref = _oracle(p, ic["m"], eps, G)
+    assert np.all(np.isfinite(got))
+    a, g, r = got[:, :3], gen[:, :3], ref[:, :3]
+    if precision == 0:
+        assert np.max(np.abs(got - ref)) <= 1e-12 * np.max(np.abs(ref))
+        assert np.max(np.abs(got - gen)) <= 1e-13 * np.max(np.abs(ref))
+    else:
+        rms = lambda x, y: np.sqrt(np.mean(np.sum((x - y) ** 2, 1)) / np.mean(np.sum(y ** 2, 1)))
+        assert rms(a, r) < 1e-6
+        assert rms(a, g) < 1e-6
+        assert np.max(np.abs(got[:, 3] / ref[:, 3] - 1)) < 1e-5
