@@ -28,8 +28,9 @@ larger than L2, so no flush is needed between steps.
                on a bounded sample (see 'sample')
 
 --impl reference times only the reference's CPU build on the same workload.
-Under torchrun (N > 1) every rank runs an independent replica (the path is
-data-parallel over independent simulations here); rank 0 prints.
+Under torchrun (N > 1) the ranks share ONE simulation of the same workload
+(cudasph_b200.sharded: SPH leaf ranges and gravity work items per rank, three
+NCCL all-reduces per step; strong scaling); rank 0 prints.
 """
 from __future__ import annotations
 
@@ -437,7 +438,7 @@ def run_ours(args, rank, world):
         t = torch.tensor([ms_step], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_step = float(t.item())
-    value = world * n * 1000.0 / ms_step
+    value = n * 1000.0 / ms_step
     stats = sim.system_statistics()
     gms, gl = ph["gravity"]
     grav_ms = gms / max(gl, 1)
@@ -448,7 +449,7 @@ def run_ours(args, rank, world):
            "vs_baseline": None, "dtype": "f64" if args.fp64_only else "f32+f64", "data": "synthetic (seeded)",
            "config": {"workload": workload_name(n), "n_particles": n, "precision": "fp64" if args.fp64_only else
                       "mixed (FP32 gravity pair terms, FP64 SPH pair terms)", "l2": "state (~%.0f MB) larger than L2; no flush" % (n * 500 / 1e6),
-                      "parallelism": "replicas" if world > 1 else "single GPU"},
+                      "parallelism": "single GPU"},
            "gpu_launches": int(launches),
            "phase_ms_per_step": {k: round(v[0] / args.steps, 4) for k, v in ph.items()},
            "device_flags": flags}
@@ -556,6 +557,107 @@ def run_ours(args, rank, world):
     return out
 
 
+def run_sharded(args, rank, world):
+    """N > 1 ranks under torchrun: ONE simulation of n particles sharded over
+    the ranks (cudasph_b200.sharded: leaf ranges of the SPH loops and shares
+    of the gravity work items per rank, three NCCL all-reduces per step), so
+    the total work is fixed as N grows (strong scaling).  Device time: CUDA
+    events on each rank's context stream around the timed steps (collectives
+    included), max over ranks."""
+    import torch
+    import torch.distributed as dist
+    from cudasph_b200 import _capi
+    from cudasph_b200.sharded import ShardedSimulation
+    from cudasph_b200.simulation import make_params
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    n = args.n
+    ic = workload_ic(n)
+    kw = dict(WORKLOAD_PARAMS, precision=0 if args.fp64_only else 1)
+    L = _capi.lib()
+    peak = L.cudasph_fma_peak(0 if args.fp64_only else 1, 1024 if args.fp64_only else 4096, None)
+
+    sim = ShardedSimulation(ic, make_params(**kw), rank, world, device=dev)
+    sim.step(args.warmup)
+    sim.synchronize()
+    dist.barrier()
+    st = sim.torch_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sim.reset_counters()
+    sim.set_profiling(True)
+    with ClockSampler(gpu_uuid()) as clk:
+        e0.record(st)
+        sim.step(args.steps)
+        e1.record(st)
+        e1.synchronize()
+        dist.barrier()
+    clocks = clk.summary()
+    ph = sim.phase_times()
+    sim.set_profiling(False)
+    launches = sim.kernel_launches()
+    flags = sim.device_status()
+    ms_local = e0.elapsed_time(e1) / args.steps
+    t = torch.tensor([ms_local], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_step = float(t.item())
+    gms, gl = ph["gravity"]
+    grav_ms = gms / max(gl, 1)
+    phase_sum = sum(v[0] for v in ph.values()) / args.steps
+
+    # end to end through the public API with host buffers: every rank copies
+    # the whole state in (its replica), steps, and copies the state out
+    e2e = None
+    if args.e2e_steps > 0:
+        ins = ("x", "y", "z", "range", "vx", "vy", "vz", "m", "u", "mu", "ax", "ay", "az", "du")
+        outs = ins + ("rho", "P")
+        host = {k: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy() for k in ins}
+        for k in ins:
+            host[k][:] = sim.get(k)
+        dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            sim.set_state(host)
+            sim.step()
+            got = sim.get_state(outs)
+            for k in ins:
+                host[k][:] = got[k]
+        wall = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device="cuda")
+        dist.all_reduce(wall, op=dist.ReduceOp.MAX)
+        e2e = {"value": n * args.e2e_steps / float(wall.item()), "unit": UNIT, "h2d_bytes_per_step": 8 * n * len(ins),
+               "d2h_bytes_per_step": 8 * n * len(outs), "steps": args.e2e_steps,
+               "api": "ShardedSimulation set_state / step / get_state (C ABI), pinned host buffers, wall clock, "
+                      "max over ranks, per rank"}
+    sim.close()
+    if rank != 0:
+        return None
+    flops = 20.0 * n * n / world
+    out = {"metric": METRIC, "value": n * 1000.0 / ms_step, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "strong",
+           "vs_baseline": None, "dtype": "f64" if args.fp64_only else "f32+f64", "data": "synthetic (seeded)",
+           "config": {"workload": workload_name(n), "n_particles": n,
+                      "precision": "fp64" if args.fp64_only else "mixed (FP32 gravity pair terms, FP64 SPH pair terms)",
+                      "l2": "state (~%.0f MB) larger than L2; no flush" % (n * 500 / 1e6),
+                      "parallelism": f"shard{world}: SPH leaf ranges + gravity work items per rank, replicated "
+                                     f"state, 3 NCCL all-reduces per step"},
+           "gpu_launches": int(launches),
+           "phase_ms_per_step": {k: round(v[0] / args.steps, 4) for k, v in ph.items()},
+           "exchange_and_gaps_ms_per_step": round(ms_local - phase_sum, 4),
+           "device_flags": flags,
+           "roofline": {"kernel": "gravity_fp64_plummer" if args.fp64_only else "gravity_mixed_plummer",
+                        "bound": "fp64_pipe" if args.fp64_only else "fp32_pipe",
+                        "achieved": flops / (grav_ms * 1e-3) / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
+                        "frac": flops / (grav_ms * 1e-3) / peak,
+                        "traffic": traffic_from_profiles("gravity_mixed_plummer", n) if not args.fp64_only else None,
+                        "peak_source": "FMA-chain probe measured in this run", "flops_per_launch": flops,
+                        "launch_ms": grav_ms, "note": "rank 0's share (1/N of the pairs)"}}
+    if clocks:
+        out["clocks"] = clocks
+    if e2e:
+        out["e2e"] = e2e
+    return out
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return None
@@ -597,6 +699,8 @@ def main():
     ap.add_argument("--cpu-grav-targets", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false")
+    ap.add_argument("--sharded", action="store_true",
+                    help="run the sharded multi-GPU path also at N = 1 (a one-rank NCCL process group)")
     ap.add_argument("--drift-steps", type=int, default=0,
                     help="instead of the bench line, measure energy drift over this many steps (mixed vs FP64)")
     ap.add_argument("--large", action="store_true",
@@ -613,16 +717,26 @@ def main():
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
-    if world > 1 and args.impl == "ours":
+    sharded = args.impl == "ours" and (world > 1 or args.sharded)
+    if sharded:
         import torch
         import torch.distributed as dist
         from datetime import timedelta
-        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        local = int(os.environ.get("LOCAL_RANK", 0))
+        torch.cuda.set_device(local)
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        os.environ.setdefault("MASTER_PORT", "29511")
+        dist.init_process_group("nccl", rank=rank, world_size=world, timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
     try:
-        out = run_ours(args, rank, world) if args.impl == "ours" else run_reference(args, rank, world)
+        if args.impl != "ours":
+            out = run_reference(args, rank, world)
+        elif sharded:
+            out = run_sharded(args, rank, world)
+        else:
+            out = run_ours(args, rank, world)
     finally:
-        if world > 1 and args.impl == "ours":
+        if sharded:
             import torch.distributed as dist
             dist.destroy_process_group()
     if out is not None and rank == 0:

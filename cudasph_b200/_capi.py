@@ -72,7 +72,7 @@ def lib():
     L.cudasph_get_time.argtypes = [vp, C.POINTER(dp), C.POINTER(dp)]
     L.cudasph_get_neighbours.argtypes = [vp, vp, vp, vp]
     L.cudasph_get_solve_evals.argtypes = [vp, vp]
-    for name in ("sort", "predict", "build_tree", "solve_range", "find_ngb", "density", "pressure", "hydro",
+    for name in ("begin_step", "shard_pack", "shard_unpack", "sort", "predict", "build_tree", "solve_range", "find_ngb", "density", "pressure", "hydro",
                  "sph_accelerations", "gravity", "finish", "kick", "step", "synchronize", "reset_counters"):
         getattr(L, "cudasph_" + name).argtypes = [vp]
     L.cudasph_steps.argtypes = [vp, ip]
@@ -98,6 +98,11 @@ def lib():
     L.cudasph_adjoint_set_dt.argtypes = [vp, dp]
     L.cudasph_adjoint_get_dt.argtypes = [vp, C.POINTER(dp)]
     L.cudasph_adjoint.argtypes = [vp]
+    L.cudasph_shard_range.argtypes = [C.c_longlong, ip, ip, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+    L.cudasph_set_shard.argtypes = [vp, ip, ip]
+    L.cudasph_get_shard.argtypes = [vp, vp, vp, vp, vp]
+    L.cudasph_device_buffer.argtypes = [vp, ip, C.POINTER(vp), C.POINTER(C.c_longlong)]
+    L.cudasph_get_stream.argtypes = [vp, C.POINTER(vp)]
     _lib = L
     return L
 

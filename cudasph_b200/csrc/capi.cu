@@ -20,16 +20,20 @@ int morton_keys(int n, const double4 *pos, const double *x, const double *y, con
 int tree_layout(int n, TreeView *t);
 int build_tree(const TreeView &t, const double4 *pos, float4 *lo, float4 *hi, cudaStream_t st);
 int launch_solve_range(const TreeView &t, double4 *pos, int *nevals, unsigned *flags, const sph_params &p,
-                       int *n_ngb, int *list, double *dcache, int cap, cudaStream_t st);
+                       int *n_ngb, int *list, double *dcache, int cap, int leaf0, int leaf1, cudaStream_t st);
 int launch_find_ngb(const TreeView &t, const double4 *pos, int *n_ngb, int *list, int cap, unsigned *flags,
-                    cudaStream_t st);
+                    int leaf0, int leaf1, cudaStream_t st);
 int launch_density(const HydroArgs &a, cudaStream_t st);
 int launch_pressure(int n, double4 *hyd, int eos_mode, double gamma, unsigned *flags, cudaStream_t st);
 int launch_hydro(const HydroArgs &a, cudaStream_t st);
 int launch_density_mixed(const HydroArgs &a, cudaStream_t st);
 int launch_hydro_mixed(const HydroArgs &a, cudaStream_t st);
 int launch_gravity(int n, const double4 *src, const double *h2src, double4 *out, int soft_mode, double eps, double G,
-                   int precision, const int *mass_mixed, cudaStream_t st);
+                   int precision, const int *mass_mixed, int rank, int world, cudaStream_t st);
+int launch_shard_pack(int n, int s0, int s1, const double4 *pos, const double4 *hyd, const double4 *dd,
+                      const int *n_ngb, double4 *xbuf, cudaStream_t st);
+int launch_shard_unpack(int n, const double4 *xbuf, double4 *pos, double4 *hyd, double4 *dd, int *n_ngb,
+                        cudaStream_t st);
 int launch_pack_sources(int n, const double4 *pos, const double4 *vel, double4 *src, double *h2, int *mass_mixed,
                         cudaStream_t st);
 int launch_predict(int n, double4 *pos, double4 *vel, double4 *hyd, const double4 *dots, double4 *old,
@@ -106,6 +110,11 @@ struct sph_ctx {
   double4 *pre_acc = nullptr, *xb = nullptr, *vb = nullptr, *ab = nullptr, *vpb = nullptr, *vpup = nullptr;
   double *rhob = nullptr, *Pb = nullptr, *omb = nullptr, *psib = nullptr, *divb = nullptr, *curlb = nullptr;
   double *cb = nullptr, *bb = nullptr, *prb = nullptr, *rho_ext = nullptr, *asc = nullptr, *apart = nullptr;
+  // sharding (cudasph_set_shard): this context computes shard `rank` of
+  // `world` of the leaf-parallel SPH loops and of the gravity work; xbuf is
+  // the exchange buffer of the SPH results (2 double4 per particle)
+  int rank = 0, world = 1;
+  double4 *xbuf = nullptr;
 };
 
 static void drop_graphs(sph_ctx *c);
@@ -200,6 +209,14 @@ FieldRef field_ref(sph_ctx *c, int field) {
   return r;
 }
 
+// this context's leaves: all of them, or its shard's contiguous range
+void shard_leaves(const sph_ctx *c, int &leaf0, int &leaf1) {
+  long long lo, hi;
+  shard_range(c->tree.count[0], c->rank, c->world, lo, hi);
+  leaf0 = (int)lo;
+  leaf1 = (int)hi;
+}
+
 HydroArgs hydro_args(sph_ctx *c) {
   Fields &F = c->f[c->cur];
   HydroArgs a;
@@ -211,6 +228,7 @@ HydroArgs hydro_args(sph_ctx *c) {
   a.alpha = c->p.av_alpha; a.beta = c->p.av_beta; a.gamma = c->p.gamma;
   a.use_psi = use_psi(c->p);
   a.jside = 1;
+  shard_leaves(c, a.leaf0, a.leaf1);
   return a;
 }
 
@@ -251,7 +269,7 @@ extern "C" int cudasph_destroy(sph_ctx *c) {
   }
   cudaFree(c->old); cudaFree(c->n_ngb); cudaFree(c->nevals); cudaFree(c->list); cudaFree(c->dcache);
   cudaFree(c->tlo); cudaFree(c->thi); cudaFree(c->keys); cudaFree(c->vals); cudaFree(c->sort_scratch);
-  cudaFree(c->bbox_part); cudaFree(c->box4); cudaFree(c->gsrc); cudaFree(c->gh2); cudaFree(c->mass_mixed); cudaFree(c->flags);
+  cudaFree(c->bbox_part); cudaFree(c->box4); cudaFree(c->gsrc); cudaFree(c->gh2); cudaFree(c->mass_mixed); cudaFree(c->xbuf); cudaFree(c->flags);
   cudaFree(c->sc); cudaFree(c->fin_part); cudaFree(c->flat); cudaFree(c->slot_of);
   cudaFree(c->pre_acc); cudaFree(c->xb); cudaFree(c->vb); cudaFree(c->ab); cudaFree(c->vpb); cudaFree(c->vpup);
   cudaFree(c->rhob); cudaFree(c->Pb); cudaFree(c->omb); cudaFree(c->psib); cudaFree(c->divb); cudaFree(c->curlb);
@@ -559,8 +577,10 @@ extern "C" int cudasph_solve_range(sph_ctx *c) {
   }
   SPH_CUDA_TRY(cudaSetDevice(c->device));
   PhaseScope ps(c, SPH_PH_SOLVE);
+  int leaf0, leaf1;
+  shard_leaves(c, leaf0, leaf1);
   LAUNCHED(launch_solve_range(c->tree, c->f[c->cur].pos, c->nevals, c->flags, c->p, c->n_ngb, c->list, c->dcache,
-                              c->list_cap, c->st));
+                              c->list_cap, leaf0, leaf1, c->st));
   // the solve writes the neighbour lists at the final ranges (find_ngb fused)
   c->lists_ok = true;
   c->density_ok = false;
@@ -577,7 +597,9 @@ extern "C" int cudasph_find_ngb(sph_ctx *c) {
   if (c->lists_ok) return SPH_OK;  // already written by the h solve at these ranges
   SPH_CUDA_TRY(cudaSetDevice(c->device));
   PhaseScope ps(c, SPH_PH_FIND);
-  LAUNCHED(launch_find_ngb(c->tree, c->f[c->cur].pos, c->n_ngb, c->list, c->list_cap, c->flags, c->st));
+  int leaf0, leaf1;
+  shard_leaves(c, leaf0, leaf1);
+  LAUNCHED(launch_find_ngb(c->tree, c->f[c->cur].pos, c->n_ngb, c->list, c->list_cap, c->flags, leaf0, leaf1, c->st));
   c->lists_ok = true;
   SPH_CUDA_TRY(cudaGetLastError());
   return SPH_OK;
@@ -612,6 +634,8 @@ extern "C" int cudasph_hydro(sph_ctx *c) {
   PhaseScope ps(c, SPH_PH_HYDRO);
   Fields &F = c->f[c->cur];
   SPH_CUDA_TRY(cudaMemsetAsync(F.dots, 0, sizeof(double4) * c->n, c->st));
+  // a shard writes the signal speeds of its own particles only; zeros elsewhere make the sum over shards exact
+  if (c->world > 1) SPH_CUDA_TRY(cudaMemsetAsync(F.vsig, 0, sizeof(double) * c->n, c->st));
   HydroArgs a = hydro_args(c);
   if (c->p.precision == SPH_PREC_MIXED && (c->p.mixed_sph & 2)) LAUNCHED(launch_hydro_mixed(a, c->st));
   else LAUNCHED(launch_hydro(a, c->st));
@@ -637,7 +661,7 @@ extern "C" int cudasph_gravity(sph_ctx *c) {
   Fields &F = c->f[c->cur];
   LAUNCHED(launch_pack_sources(c->n, F.pos, F.vel, c->gsrc, c->gh2, c->mass_mixed, c->st));
   LAUNCHED(launch_gravity(c->n, c->gsrc, c->gh2, F.grav, c->p.soft_mode, c->p.eps, c->p.G, c->p.precision,
-                          c->mass_mixed, c->st));
+                          c->mass_mixed, c->rank, c->world, c->st));
   SPH_CUDA_TRY(cudaGetLastError());
   return SPH_OK;
 }
@@ -680,6 +704,11 @@ static int step_body(sph_ctx *c);
 // (buffer flip, phase validity) is then repeated by hand on every replay.
 extern "C" int cudasph_step(sph_ctx *c) {
   if (!c) return SPH_ERR_ARG;
+  if (c->world > 1) {
+    sph_internal_set_error("cudasph_step: a sharded context is stepped phase by phase with the exchanges "
+                           "between them (cudasph_shard_pack / unpack, sums of dots, vsig and grav)");
+    return SPH_ERR_STATE;
+  }
   const bool graphable = c->use_graph && !c->need_sort && c->p.sort_every == 1 && !c->profiling && !c->keep;
   if (!graphable) return step_body(c);
   SPH_CUDA_TRY(cudaSetDevice(c->device));
@@ -723,11 +752,16 @@ extern "C" int cudasph_set_graph(sph_ctx *c, int on) {
   return SPH_OK;
 }
 
+extern "C" int cudasph_begin_step(sph_ctx *c) {
+  if (!c) return SPH_ERR_ARG;
+  c->iteration++;
+  if (c->need_sort || (c->p.sort_every > 0 && c->iteration % c->p.sort_every == 0)) return cudasph_sort(c);
+  return SPH_OK;
+}
+
 static int step_body(sph_ctx *c) {
   int rc;
-  c->iteration++;
-  if (c->need_sort || (c->p.sort_every > 0 && c->iteration % c->p.sort_every == 0))
-    if ((rc = cudasph_sort(c))) return rc;
+  if ((rc = cudasph_begin_step(c))) return rc;
   if (c->keep) {
     // the adjoint needs the accelerations the predictor uses (a0, du0)
     SPH_CUDA_TRY(cudaSetDevice(c->device));
@@ -825,6 +859,10 @@ extern "C" long long cudasph_kernel_launches(const sph_ctx *c) { return c ? c->l
 // ------------------------------- the adjoint --------------------------------
 extern "C" int cudasph_set_keep(sph_ctx *c, int on) {
   if (!c) return SPH_ERR_ARG;
+  if (on && c->world > 1) {
+    sph_internal_set_error("cudasph_set_keep: the adjoint runs on an unsharded context");
+    return SPH_ERR_STATE;
+  }
   SPH_CUDA_TRY(cudaSetDevice(c->device));
   if (on && !c->pre_acc) {
     const int n = c->n;
@@ -938,6 +976,87 @@ extern "C" int cudasph_adjoint(sph_ctx *c) {
   SPH_CUDA_TRY(cudaMemsetAsync(c->rho_ext, 0, sizeof(double) * c->n, c->st));
   SPH_CUDA_TRY(cudaGetLastError());
   c->kept = false;
+  return SPH_OK;
+}
+
+// ------------------------------- sharding ------------------------------------
+extern "C" int cudasph_shard_range(long long count, int rank, int world, long long *lo, long long *hi) {
+  if (!lo || !hi || count < 0 || world < 1 || rank < 0 || rank >= world) return SPH_ERR_ARG;
+  shard_range(count, rank, world, *lo, *hi);
+  return SPH_OK;
+}
+
+extern "C" int cudasph_set_shard(sph_ctx *c, int rank, int world) {
+  if (!c || world < 1 || rank < 0 || rank >= world) return SPH_ERR_ARG;
+  if (c->keep && world > 1) {
+    sph_internal_set_error("cudasph_set_shard: the adjoint runs on an unsharded context");
+    return SPH_ERR_STATE;
+  }
+  SPH_CUDA_TRY(cudaSetDevice(c->device));
+  SPH_CUDA_TRY(cudaStreamSynchronize(c->st));
+  if (!c->xbuf) {
+    int rc = dalloc(&c->xbuf, 2 * (size_t)c->n);
+    if (rc) return rc;
+  }
+  drop_graphs(c);
+  c->rank = rank;
+  c->world = world;
+  c->lists_ok = c->density_ok = false;
+  return SPH_OK;
+}
+
+extern "C" int cudasph_get_shard(sph_ctx *c, int *rank, int *world, int *leaf0, int *leaf1) {
+  if (!c) return SPH_ERR_ARG;
+  if (rank) *rank = c->rank;
+  if (world) *world = c->world;
+  int l0, l1;
+  shard_leaves(c, l0, l1);
+  if (leaf0) *leaf0 = l0;
+  if (leaf1) *leaf1 = l1;
+  return SPH_OK;
+}
+
+extern "C" int cudasph_shard_pack(sph_ctx *c) {
+  if (!c) return SPH_ERR_ARG;
+  if (!c->xbuf || !c->density_ok) return SPH_ERR_STATE;
+  SPH_CUDA_TRY(cudaSetDevice(c->device));
+  Fields &F = c->f[c->cur];
+  int l0, l1;
+  shard_leaves(c, l0, l1);
+  const int s0 = l0 * kLeaf, s1 = min(l1 * kLeaf, c->n);
+  LAUNCHED(launch_shard_pack(c->n, s0, s1, F.pos, F.hyd, F.dd, c->n_ngb, c->xbuf, c->st));
+  SPH_CUDA_TRY(cudaGetLastError());
+  return SPH_OK;
+}
+
+extern "C" int cudasph_shard_unpack(sph_ctx *c) {
+  if (!c) return SPH_ERR_ARG;
+  if (!c->xbuf) return SPH_ERR_STATE;
+  SPH_CUDA_TRY(cudaSetDevice(c->device));
+  Fields &F = c->f[c->cur];
+  LAUNCHED(launch_shard_unpack(c->n, c->xbuf, F.pos, F.hyd, F.dd, c->n_ngb, c->st));
+  SPH_CUDA_TRY(cudaGetLastError());
+  return SPH_OK;
+}
+
+extern "C" int cudasph_device_buffer(sph_ctx *c, int which, void **ptr, long long *doubles) {
+  if (!c || !ptr || !doubles) return SPH_ERR_ARG;
+  Fields &F = c->f[c->cur];
+  switch (which) {
+    case SPH_BUF_EXCHANGE:
+      if (!c->xbuf) return SPH_ERR_STATE;
+      *ptr = c->xbuf; *doubles = 8LL * c->n; break;
+    case SPH_BUF_DOTS: *ptr = F.dots; *doubles = 4LL * c->n; break;
+    case SPH_BUF_VSIG: *ptr = F.vsig; *doubles = c->n; break;
+    case SPH_BUF_GRAV: *ptr = F.grav; *doubles = 4LL * c->n; break;
+    default: return SPH_ERR_ARG;
+  }
+  return SPH_OK;
+}
+
+extern "C" int cudasph_get_stream(sph_ctx *c, void **stream) {
+  if (!c || !stream) return SPH_ERR_ARG;
+  *stream = (void *)c->st;
   return SPH_OK;
 }
 

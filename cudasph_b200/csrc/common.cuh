@@ -47,6 +47,7 @@ struct Fields {
 // arguments of the density / hydro kernels (both precision forms)
 struct HydroArgs {
   int n, nleaf, cap;
+  int leaf0, leaf1;  // leaves [leaf0, leaf1) processed by this launch (a shard's range, or all)
   const double4 *pos, *vel;
   double4 *hyd, *dd, *dots;
   double *vsig;
@@ -132,6 +133,14 @@ __device__ __forceinline__ void sym_item(long long item, int nt, int &b, int &t_
   b = lo;
   t_lo = b + 1 + (int)(item - sym_first(b, nt)) * kSymChunk;
   t_hi = min(t_lo + kSymChunk, nt);
+}
+
+// Contiguous balanced split of [0, count) over `world` shards: shard `rank`
+// owns [count * rank / world, count * (rank + 1) / world).
+__host__ __device__ __forceinline__ void shard_range(long long count, int rank, int world, long long &lo,
+                                                     long long &hi) {
+  lo = count * rank / world;
+  hi = count * (rank + 1) / world;
 }
 
 }  // namespace sph

@@ -90,11 +90,11 @@ __device__ __noinline__ void spline_near(R dx, R dy, R dz, R r2, R mj, R hi2, R 
 template <int SOFT, int R>
 __global__ void __launch_bounds__(kGThreads) k_grav_f64(int n, const double4 *__restrict__ src,
                                                         const double *__restrict__ h2src, double4 *__restrict__ out,
-                                                        double eps2, double G, int tile) {
+                                                        double eps2, double G, int tile, int block0) {
   __shared__ double4 sj[kGThreads];
   __shared__ double sh[SOFT == SPH_SOFT_SPLINE ? kGThreads : 1];
   const int t = threadIdx.x;
-  const int i0 = blockIdx.x * kGThreads * R;
+  const int i0 = (blockIdx.x + block0) * kGThreads * R;
   const int jlo = tile > 0 ? (i0 / tile) * tile : 0;
   const int jhi = tile > 0 ? min(jlo + tile, n) : n;
   double xi[R], yi[R], zi[R], hi2[R], ax[R], ay[R], az[R], pot[R];
@@ -177,11 +177,11 @@ __device__ __forceinline__ void kahan_add(float &hi, float &lo, float v) {
 template <int SOFT, int R>
 __global__ void __launch_bounds__(kGThreads) k_grav_f32(int n, const double4 *__restrict__ src,
                                                         const double *__restrict__ h2src, double4 *__restrict__ out,
-                                                        float eps2, double G) {
+                                                        float eps2, double G, int block0) {
   __shared__ float4 sj[kGThreads];
   __shared__ float sh[SOFT == SPH_SOFT_SPLINE ? kGThreads : 1];
   const int t = threadIdx.x;
-  const int i0 = blockIdx.x * kGThreads * R;
+  const int i0 = (blockIdx.x + block0) * kGThreads * R;
   const double4 anc = src[min(i0, n - 1)];
   float xi[R], yi[R], zi[R], hi2[R];
   float ahi[R][4], alo[R][4];
@@ -302,10 +302,10 @@ __global__ void __launch_bounds__(kGThreads) k_grav_f32(int n, const double4 *__
 template <int RP>  // i-particle pairs per thread
 __global__ void __launch_bounds__(kGThreads) k_grav_f32x2_plummer(int n, const double4 *__restrict__ src,
                                                                   double4 *__restrict__ out, float eps2, double G,
-                                                                  int tile) {
+                                                                  int tile, int block0) {
   __shared__ ulonglong2 sj[kGThreads][2];
   const int t = threadIdx.x;
-  const int i0 = blockIdx.x * kGThreads * 2 * RP;
+  const int i0 = (blockIdx.x + block0) * kGThreads * 2 * RP;
   const int jlo = tile > 0 ? (i0 / tile) * tile : 0;
   const int jhi = tile > 0 ? min(jlo + tile, n) : n;
   const double4 anc = src[min(i0, n - 1)];
@@ -428,12 +428,12 @@ constexpr int kSymRP = 8;
 constexpr int kSymTile = kSymWarps * 64 * kSymRP;  // 1024 i-particles per block
 
 template <bool UNI>
-__device__ __forceinline__ void sym_plummer_item(int n, int nt, const double4 *__restrict__ src,
+__device__ __forceinline__ void sym_plummer_item(long long item, int n, int nt, const double4 *__restrict__ src,
                                                  double4 *__restrict__ out, float eps2, double G,
                                                  float (&red)[2][kSymWarps][4][32],
                                                  double (&iacc)[2 * kSymRP * 4][kSymWarps * 32]) {
   int b, t_lo, t_hi;
-  sym_item(blockIdx.x, nt, b, t_lo, t_hi);
+  sym_item(item, nt, b, t_lo, t_hi);
   const int j_lo = t_lo * kSymTile, j_hi = min(t_hi * kSymTile, n);
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nxt = (l + 1) & 31;
   const int i0 = b * kSymTile;
@@ -556,16 +556,19 @@ __device__ __forceinline__ void sym_plummer_item(int n, int nt, const double4 *_
   }
 }
 
-// mass_mixed: device word, 0 when all masses are equal (nullptr: general form)
+// mass_mixed: device word, 0 when all masses are equal (nullptr: general form);
+// block b runs work item item0 + b
 __global__ void __launch_bounds__(kSymWarps * 32, 4) k_grav_sym_plummer(int n, int nt, const double4 *__restrict__ src,
                                                                          double4 *__restrict__ out, float eps2,
-                                                                         double G, const int *__restrict__ mass_mixed) {
+                                                                         double G, const int *__restrict__ mass_mixed,
+                                                                         long long item0) {
   __shared__ float red[2][kSymWarps][4][32];
   __shared__ double iacc[2 * kSymRP * 4][kSymWarps * 32];  // [i-slot * 4 + component][thread]
+  const long long item = item0 + blockIdx.x;
   if (mass_mixed != nullptr && __ldg(mass_mixed) == 0)
-    sym_plummer_item<true>(n, nt, src, out, eps2, G, red, iacc);
+    sym_plummer_item<true>(item, n, nt, src, out, eps2, G, red, iacc);
   else
-    sym_plummer_item<false>(n, nt, src, out, eps2, G, red, iacc);
+    sym_plummer_item<false>(item, n, nt, src, out, eps2, G, red, iacc);
 }
 
 // ------------------- FP64, symmetric pair form ------------------------------
@@ -583,10 +586,11 @@ constexpr int kSym64R = 8;
 static_assert(kSym64Warps * 32 * kSym64R == kSymTile, "the FP64 form shares the tile layout");
 
 template <bool UNI>
-__device__ __forceinline__ void sym_f64_item(int n, int nt, const double4 *__restrict__ src, double4 *__restrict__ out,
-                                             double eps2, double G, double (&red)[2][kSym64Warps][4][32]) {
+__device__ __forceinline__ void sym_f64_item(long long item, int n, int nt, const double4 *__restrict__ src,
+                                             double4 *__restrict__ out, double eps2, double G,
+                                             double (&red)[2][kSym64Warps][4][32]) {
   int b, t_lo, t_hi;
-  sym_item(blockIdx.x, nt, b, t_lo, t_hi);
+  sym_item(item, nt, b, t_lo, t_hi);
   const int j_lo = t_lo * kSymTile, j_hi = min(t_hi * kSymTile, n);
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nxt = (l + 1) & 31;
   const int ib = b * kSymTile + w * 32 * kSym64R + l;
@@ -677,34 +681,60 @@ __device__ __forceinline__ void sym_f64_item(int n, int nt, const double4 *__res
 
 __global__ void __launch_bounds__(kSym64Warps * 32) k_grav_sym_f64(int n, int nt, const double4 *__restrict__ src,
                                                                   double4 *__restrict__ out, double eps2, double G,
-                                                                  const int *__restrict__ mass_mixed) {
+                                                                  const int *__restrict__ mass_mixed, long long item0) {
   __shared__ double red[2][kSym64Warps][4][32];
+  const long long item = item0 + blockIdx.x;
   if (mass_mixed != nullptr && __ldg(mass_mixed) == 0)
-    sym_f64_item<true>(n, nt, src, out, eps2, G, red);
+    sym_f64_item<true>(item, n, nt, src, out, eps2, G, red);
   else
-    sym_f64_item<false>(n, nt, src, out, eps2, G, red);
+    sym_f64_item<false>(item, n, nt, src, out, eps2, G, red);
 }
 
-// src = {x, y, z, m} per particle; h2src = range^2 (spline mode only)
+// blocks [lo, hi) of a one-sided or symmetric launch (nothing when empty)
+struct Span {
+  long long lo, hi;
+  unsigned grid() const { return (unsigned)(hi - lo); }
+  bool empty() const { return hi <= lo; }
+};
+static Span shard_span(long long count, int rank, int world) {
+  Span sp;
+  shard_range(count, rank, world, sp.lo, sp.hi);
+  return sp;
+}
+
+// src = {x, y, z, m} per particle; h2src = range^2 (spline mode only).
+// Shard `rank` of `world` (world > 1) computes its contiguous share of the
+// one-sided blocks (diagonal tiles, or all pairs for small n / spline
+// softening) and of the symmetric work items into `out`, which it zeroes
+// first: the element-wise sum of the shards' outputs is the whole sum.
 int launch_gravity(int n, const double4 *src, const double *h2src, double4 *out, int soft_mode, double eps, double G,
-                   int precision, const int *mass_mixed, cudaStream_t st) {
+                   int precision, const int *mass_mixed, int rank, int world, cudaStream_t st) {
   if (n <= 0) return 0;
+  if (world > 1) cudaMemsetAsync(out, 0, sizeof(double4) * n, st);
   const double eps2 = eps * eps;
+  const int nt = (n + kSymTile - 1) / kSymTile;
+  const Span items = shard_span(nt >= 2 ? sym_S(nt - 1) : 0, rank, world);
+  int launches = 0;
   if (precision == SPH_PREC_FP64) {
     constexpr int R = 2;
     static_assert(kSymTile % (kGThreads * R) == 0, "diagonal tiles must hold whole blocks");
-    const int blocks = (n + kGThreads * R - 1) / (kGThreads * R);
-    const int nt = (n + kSymTile - 1) / kSymTile;
+    const Span blocks = shard_span((n + kGThreads * R - 1) / (kGThreads * R), rank, world);
     if (soft_mode == SPH_SOFT_PLUMMER) {
-      if (nt < 2) {
-        k_grav_f64<SPH_SOFT_PLUMMER, R><<<blocks, kGThreads, 0, st>>>(n, src, h2src, out, eps2, G, 0);
-      } else {
-        k_grav_f64<SPH_SOFT_PLUMMER, R><<<blocks, kGThreads, 0, st>>>(n, src, h2src, out, eps2, G, kSymTile);
-        k_grav_sym_f64<<<(unsigned)sym_S(nt - 1), kSym64Warps * 32, 0, st>>>(n, nt, src, out, eps2, G,
-                                                                              mass_mixed);
+      // diagonal tiles one-sided (all pairs when there is a single tile), then the items above them
+      const int tile = nt < 2 ? 0 : kSymTile;
+      if (!blocks.empty()) {
+        k_grav_f64<SPH_SOFT_PLUMMER, R><<<blocks.grid(), kGThreads, 0, st>>>(n, src, h2src, out, eps2, G, tile,
+                                                                            (int)blocks.lo);
+        launches++;
       }
-    } else {
-      k_grav_f64<SPH_SOFT_SPLINE, R><<<blocks, kGThreads, 0, st>>>(n, src, h2src, out, eps2, G, 0);
+      if (!items.empty()) {
+        k_grav_sym_f64<<<items.grid(), kSym64Warps * 32, 0, st>>>(n, nt, src, out, eps2, G, mass_mixed, items.lo);
+        launches++;
+      }
+    } else if (!blocks.empty()) {
+      k_grav_f64<SPH_SOFT_SPLINE, R><<<blocks.grid(), kGThreads, 0, st>>>(n, src, h2src, out, eps2, G, 0,
+                                                                         (int)blocks.lo);
+      launches++;
     }
   } else {
     if (soft_mode == SPH_SOFT_PLUMMER) {
@@ -712,24 +742,30 @@ int launch_gravity(int n, const double4 *src, const double *h2src, double4 *out,
       // resident warps to cover the MUFU latency)
       constexpr int RP = 1;
       static_assert(kSymTile % (kGThreads * 2 * RP) == 0, "diagonal tiles must hold whole blocks");
-      const int blocks = (n + kGThreads * 2 * RP - 1) / (kGThreads * 2 * RP);
-      const int nt = (n + kSymTile - 1) / kSymTile;
-      if (nt < 2) {
-        k_grav_f32x2_plummer<RP><<<blocks, kGThreads, 0, st>>>(n, src, out, (float)eps2, G, 0);
-      } else {
-        // diagonal tiles store, the symmetric items add on top
-        k_grav_f32x2_plummer<RP><<<blocks, kGThreads, 0, st>>>(n, src, out, (float)eps2, G, kSymTile);
-        const long long items = sym_S(nt - 1);
-        k_grav_sym_plummer<<<(unsigned)items, kSymWarps * 32, 0, st>>>(n, nt, src, out, (float)eps2, G,
-                                                                         mass_mixed);
+      const Span blocks = shard_span((n + kGThreads * 2 * RP - 1) / (kGThreads * 2 * RP), rank, world);
+      // diagonal tiles store, the symmetric items add on top
+      const int tile = nt < 2 ? 0 : kSymTile;
+      if (!blocks.empty()) {
+        k_grav_f32x2_plummer<RP><<<blocks.grid(), kGThreads, 0, st>>>(n, src, out, (float)eps2, G, tile,
+                                                                     (int)blocks.lo);
+        launches++;
+      }
+      if (!items.empty()) {
+        k_grav_sym_plummer<<<items.grid(), kSymWarps * 32, 0, st>>>(n, nt, src, out, (float)eps2, G, mass_mixed,
+                                                                    items.lo);
+        launches++;
       }
     } else {
       constexpr int R = 4;
-      const int blocks = (n + kGThreads * R - 1) / (kGThreads * R);
-      k_grav_f32<SPH_SOFT_SPLINE, R><<<blocks, kGThreads, 0, st>>>(n, src, h2src, out, (float)eps2, G);
+      const Span blocks = shard_span((n + kGThreads * R - 1) / (kGThreads * R), rank, world);
+      if (!blocks.empty()) {
+        k_grav_f32<SPH_SOFT_SPLINE, R><<<blocks.grid(), kGThreads, 0, st>>>(n, src, h2src, out, (float)eps2, G,
+                                                                           (int)blocks.lo);
+        launches++;
+      }
     }
   }
-  return 1;
+  return launches;
 }
 
 // pack the gravity sources {x, y, z, m} and range^2 from the state
@@ -776,7 +812,7 @@ extern "C" int cudasph_gravity_direct(int n, const double *pos4, const double *r
     SPH_CUDA_TRY(cudaMallocAsync((void **)&h2, sizeof(double) * n, st));
     sph::k_range_sq<<<(n + 255) / 256, 256, 0, st>>>(n, range, h2);
   }
-  sph::launch_gravity(n, (const double4 *)pos4, h2, (double4 *)out4, soft_mode, eps, G, precision, nullptr, st);
+  sph::launch_gravity(n, (const double4 *)pos4, h2, (double4 *)out4, soft_mode, eps, G, precision, nullptr, 0, 1, st);
   if (h2) SPH_CUDA_TRY(cudaFreeAsync(h2, st));
   SPH_CUDA_TRY(cudaGetLastError());
   return SPH_OK;

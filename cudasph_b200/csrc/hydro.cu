@@ -26,8 +26,8 @@ __device__ __forceinline__ int leaf_max_count(int cnt) {
 }
 
 __global__ void __launch_bounds__(128) k_density(HydroArgs a) {
-  const int leaf = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (leaf >= a.nleaf) return;
+  const int leaf = a.leaf0 + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (leaf >= a.leaf1) return;
   const int lane = (int)lane_id();
   const int s = leaf * kLeaf + lane;
   const bool valid = s < a.n;
@@ -171,8 +171,8 @@ __device__ __forceinline__ void art_visc(double range_i, double range_j, double 
 // hydro_dots (dev_hydro_dots.cu:25-113) plus the j-side of every pair.
 // dots must be zero on entry (xyz accumulate); dots.w (du/dt) is stored.
 __global__ void __launch_bounds__(128) k_hydro(HydroArgs a) {
-  const int leaf = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (leaf >= a.nleaf) return;
+  const int leaf = a.leaf0 + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (leaf >= a.leaf1) return;
   const int lane = (int)lane_id();
   const int s = leaf * kLeaf + lane;
   const bool valid = s < a.n;
@@ -234,7 +234,8 @@ __global__ void __launch_bounds__(128) k_hydro(HydroArgs a) {
 }
 
 int launch_density(const HydroArgs &a, cudaStream_t st) {
-  k_density<<<(a.nleaf * 32 + 127) / 128, 128, 0, st>>>(a);
+  if (a.leaf1 <= a.leaf0) return 0;
+  k_density<<<((a.leaf1 - a.leaf0) * 32 + 127) / 128, 128, 0, st>>>(a);
   return 1;
 }
 int launch_pressure(int n, double4 *hyd, int eos_mode, double gamma, unsigned *flags, cudaStream_t st) {
@@ -242,7 +243,8 @@ int launch_pressure(int n, double4 *hyd, int eos_mode, double gamma, unsigned *f
   return 1;
 }
 int launch_hydro(const HydroArgs &a, cudaStream_t st) {
-  k_hydro<<<(a.nleaf * 32 + 127) / 128, 128, 0, st>>>(a);
+  if (a.leaf1 <= a.leaf0) return 0;
+  k_hydro<<<((a.leaf1 - a.leaf0) * 32 + 127) / 128, 128, 0, st>>>(a);
   return 1;
 }
 

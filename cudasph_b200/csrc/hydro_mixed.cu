@@ -30,8 +30,8 @@ __device__ __forceinline__ int leaf_max_count_m(int cnt) {
 }
 
 __global__ void __launch_bounds__(128) k_density_mixed(HydroArgs a) {
-  const int leaf = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (leaf >= a.nleaf) return;
+  const int leaf = a.leaf0 + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (leaf >= a.leaf1) return;
   const int lane = (int)lane_id();
   const int s = leaf * kLeaf + lane;
   const bool valid = s < a.n;
@@ -91,8 +91,8 @@ __global__ void __launch_bounds__(128) k_density_mixed(HydroArgs a) {
 }
 
 __global__ void __launch_bounds__(128) k_hydro_mixed(HydroArgs a) {
-  const int leaf = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (leaf >= a.nleaf) return;
+  const int leaf = a.leaf0 + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (leaf >= a.leaf1) return;
   const int lane = (int)lane_id();
   const int s = leaf * kLeaf + lane;
   const bool valid = s < a.n;
@@ -170,11 +170,13 @@ __global__ void __launch_bounds__(128) k_hydro_mixed(HydroArgs a) {
 }
 
 int launch_density_mixed(const HydroArgs &a, cudaStream_t st) {
-  k_density_mixed<<<(a.nleaf * 32 + 127) / 128, 128, 0, st>>>(a);
+  if (a.leaf1 <= a.leaf0) return 0;
+  k_density_mixed<<<((a.leaf1 - a.leaf0) * 32 + 127) / 128, 128, 0, st>>>(a);
   return 1;
 }
 int launch_hydro_mixed(const HydroArgs &a, cudaStream_t st) {
-  k_hydro_mixed<<<(a.nleaf * 32 + 127) / 128, 128, 0, st>>>(a);
+  if (a.leaf1 <= a.leaf0) return 0;
+  k_hydro_mixed<<<((a.leaf1 - a.leaf0) * 32 + 127) / 128, 128, 0, st>>>(a);
   return 1;
 }
 

@@ -242,6 +242,49 @@ int launch_kick(int n, double4 *vel, double4 *hyd, const double4 *dots, const do
   return 1;
 }
 
+// Exchange of the SPH results between shards.  Every particle has two
+// double4 records in xbuf: {range, rho, div, curl} and {omega, psi, n_ngb, 0}.
+// pack: the shard's own slots [s0, s1) are copied in, every other slot is
+// zeroed, so the element-wise sum of the shards' buffers holds every
+// particle's values exactly once; unpack writes the summed buffer back.
+__global__ void k_shard_pack(int n, int s0, int s1, const double4 *__restrict__ pos, const double4 *__restrict__ hyd,
+                             const double4 *__restrict__ dd, const int *__restrict__ n_ngb,
+                             double4 *__restrict__ xbuf) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  double4 a = make_double4(0, 0, 0, 0), b = make_double4(0, 0, 0, 0);
+  if (s >= s0 && s < s1) {
+    const double4 d = dd[s];
+    a = make_double4(pos[s].w, hyd[s].x, d.x, d.y);
+    b = make_double4(d.z, d.w, (double)n_ngb[s], 0.0);
+  }
+  xbuf[2 * s] = a;
+  xbuf[2 * s + 1] = b;
+}
+
+__global__ void k_shard_unpack(int n, const double4 *__restrict__ xbuf, double4 *__restrict__ pos,
+                               double4 *__restrict__ hyd, double4 *__restrict__ dd, int *__restrict__ n_ngb) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const double4 a = xbuf[2 * s], b = xbuf[2 * s + 1];
+  pos[s].w = a.x;
+  hyd[s].x = a.y;
+  dd[s] = make_double4(a.z, a.w, b.x, b.y);
+  n_ngb[s] = (int)b.z;
+}
+
+int launch_shard_pack(int n, int s0, int s1, const double4 *pos, const double4 *hyd, const double4 *dd,
+                      const int *n_ngb, double4 *xbuf, cudaStream_t st) {
+  k_shard_pack<<<(n + 255) / 256, 256, 0, st>>>(n, s0, s1, pos, hyd, dd, n_ngb, xbuf);
+  return 1;
+}
+
+int launch_shard_unpack(int n, const double4 *xbuf, double4 *pos, double4 *hyd, double4 *dd, int *n_ngb,
+                        cudaStream_t st) {
+  k_shard_unpack<<<(n + 255) / 256, 256, 0, st>>>(n, xbuf, pos, hyd, dd, n_ngb);
+  return 1;
+}
+
 int launch_permute(int n, const uint32_t *order, const Fields &src, const Fields &dst, cudaStream_t st) {
   k_permute<<<(n + 255) / 256, 256, 0, st>>>(n, order, src, dst);
   return 1;

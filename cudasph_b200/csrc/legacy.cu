@@ -28,7 +28,7 @@ int launch_density(const HydroArgs &a, cudaStream_t st);
 int launch_hydro(const HydroArgs &a, cudaStream_t st);
 int launch_invert(int n, const int *id, int *slot_of, cudaStream_t st);
 int launch_gravity(int n, const double4 *src, const double *h2src, double4 *out, int soft_mode, double eps, double G,
-                   int precision, const int *mass_mixed, cudaStream_t st);
+                   int precision, const int *mass_mixed, int rank, int world, cudaStream_t st);
 size_t radix_scratch_bytes(int n);
 int radix_sort_u64(int n, uint64_t *keys, uint32_t *vals, void *scratch, cudaStream_t st);
 }  // namespace sph
@@ -219,7 +219,7 @@ void compute_CUDA_gravity(int numBodies, sph_legacy_float4 *accel, float *pos, f
   check(cudaMalloc((void **)&h2, sizeof(double) * numBodies), "cudaMalloc");
   const int nb = (numBodies + 255) / 256;
   k_grav_in<<<nb, 256>>>(numBodies, (const float4 *)pos, (const float4 *)vel, src, h2);
-  launch_gravity(numBodies, src, h2, out, SPH_SOFT_SPLINE, 0.0, 1.0, SPH_PREC_FP64, nullptr, 0);
+  launch_gravity(numBodies, src, h2, out, SPH_SOFT_SPLINE, 0.0, 1.0, SPH_PREC_FP64, nullptr, 0, 1, 0);
   k_grav_out<<<nb, 256>>>(numBodies, out, (float4 *)accel);
   check(cudaDeviceSynchronize(), "get_CUDA_forces");
   cudaFree(src);

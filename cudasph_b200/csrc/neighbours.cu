@@ -162,6 +162,7 @@ struct SolveArgs {
   int *list;       // neighbour lists at the final range (layout of k_find_ngb)
   double *dcache;  // squared distances of the cached candidates, layout of list
   int cap;
+  int leaf0, leaf1;  // leaves processed by this launch
 };
 
 enum { kBr0 = 0, kBr1 = 1, kSolve = 2, kDone = 3 };
@@ -189,9 +190,9 @@ constexpr double kCacheMargin = 1.15;
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_solve_range(SolveArgs a) {
   __shared__ WarpSmem smem[kWarpsPerBlock];
   WarpSmem &sm = smem[threadIdx.x >> 5];
-  const int leaf = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int leaf = a.leaf0 + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const int n = a.t.n;
-  if (leaf >= a.t.count[0]) return;
+  if (leaf >= a.leaf1) return;
   const int s = leaf * kLeaf + (int)lane_id();
   const bool valid = s < n;
   double xi = 0, yi = 0, zi = 0, w = 0;
@@ -381,6 +382,7 @@ struct FindArgs {
   int *list;       // [leaf][k][lane], cap entries per lane
   int cap;
   unsigned *flags;
+  int leaf0, leaf1;  // leaves processed by this launch
 };
 
 // dev_find_ngb (dev_find_ngb.cu:13-87): every j with ds2 < range_i^2, in
@@ -390,9 +392,9 @@ struct FindArgs {
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_find_ngb(FindArgs a) {
   __shared__ WarpSmem smem[kWarpsPerBlock];
   WarpSmem &sm = smem[threadIdx.x >> 5];
-  const int leaf = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int leaf = a.leaf0 + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const int n = a.t.n;
-  if (leaf >= a.t.count[0]) return;
+  if (leaf >= a.leaf1) return;
   const int s = leaf * kLeaf + (int)lane_id();
   const bool valid = s < n;
   double xi = 0, yi = 0, zi = 0, w = 0;
@@ -431,22 +433,27 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_find_ngb(FindArgs a) {
   if (valid) a.n_ngb[s] = cnt;
 }
 
+// leaves [leaf0, leaf1) (a shard's range, or 0 and the leaf count)
 int launch_solve_range(const TreeView &t, double4 *pos, int *nevals, unsigned *flags, const sph_params &p,
-                       int *n_ngb, int *list, double *dcache, int cap, cudaStream_t st) {
+                       int *n_ngb, int *list, double *dcache, int cap, int leaf0, int leaf1, cudaStream_t st) {
   SolveArgs a;
   a.t = t; a.pos = pos; a.nevals = nevals; a.flags = flags;
   a.n_ngb = n_ngb; a.list = list; a.dcache = dcache; a.cap = cap;
   a.n_target = p.n_target; a.rel_err = p.rel_err; a.f_scale = p.f_scale; a.max_iter = p.max_iter;
-  const int warps = t.count[0];
+  a.leaf0 = leaf0; a.leaf1 = leaf1;
+  const int warps = leaf1 - leaf0;
+  if (warps <= 0) return 0;
   k_solve_range<<<(warps + kWarpsPerBlock - 1) / kWarpsPerBlock, kWarpsPerBlock * 32, 0, st>>>(a);
   return 1;
 }
 
 int launch_find_ngb(const TreeView &t, const double4 *pos, int *n_ngb, int *list, int cap, unsigned *flags,
-                    cudaStream_t st) {
+                    int leaf0, int leaf1, cudaStream_t st) {
   FindArgs a;
   a.t = t; a.pos = pos; a.n_ngb = n_ngb; a.list = list; a.cap = cap; a.flags = flags;
-  const int warps = t.count[0];
+  a.leaf0 = leaf0; a.leaf1 = leaf1;
+  const int warps = leaf1 - leaf0;
+  if (warps <= 0) return 0;
   k_find_ngb<<<(warps + kWarpsPerBlock - 1) / kWarpsPerBlock, kWarpsPerBlock * 32, 0, st>>>(a);
   return 1;
 }

@@ -38,6 +38,7 @@ def make_params(**kw) -> _capi.Params:
 class Simulation:
     def __init__(self, ic: dict, params: _capi.Params, device: int = 0):
         self.n = int(np.asarray(ic["x"]).size)
+        self.device = device
         self.params = params
         h = C.c_void_p()
         check(lib().cudasph_create(C.byref(params), self.n, device, C.byref(h)), "cudasph_create")

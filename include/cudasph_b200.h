@@ -155,6 +155,9 @@ int cudasph_gravity(sph_ctx *ctx);           /* sph_grav_kernel.cu:179 */
 int cudasph_finish(sph_ctx *ctx);            /* a += g, diagnostics, timestep (step.cpp:96-127) */
 int cudasph_kick(sph_ctx *ctx);              /* step.cpp:128-134 */
 int cudasph_step(sph_ctx *ctx);              /* the whole step */
+/* the step's opening when it is driven phase by phase: count the step and
+ * re-sort when due (every sort_every steps, or after positions were set) */
+int cudasph_begin_step(sph_ctx *ctx);
 /* Replay steady steps (sorted every step, profiling and keep off) from a
  * captured CUDA graph: one graph launch per step instead of ~45 launches.
  * Changing parameters drops the captured graphs. */
@@ -183,6 +186,38 @@ int cudasph_phase_times(sph_ctx *ctx, double *ms /* SPH_NPHASES */, int *launche
 int cudasph_reset_counters(sph_ctx *ctx);
 /* kernels launched by this context since the last reset */
 long long cudasph_kernel_launches(const sph_ctx *ctx);
+
+/* ---------------------------------------------------------------------- */
+/* sharding over several GPUs (no counterpart in the reference, which runs */
+/* one GPU).  Every rank holds a whole replica of the state; a context     */
+/* given shard `rank` of `world` runs the leaf-parallel SPH loops (h solve */
+/* + lists, density, hydro) over its contiguous range of tree leaves and   */
+/* its contiguous share of the gravity blocks and work items.  The caller  */
+/* steps it phase by phase (cudasph_step refuses a sharded context) and    */
+/* sums three buffers over the ranks (e.g. an NCCL all-reduce on the       */
+/* context's stream, cudasph_get_stream):                                  */
+/*   sort, predict, build_tree, solve_range, density, shard_pack,          */
+/*   SUM(SPH_BUF_EXCHANGE), shard_unpack, pressure, hydro,                 */
+/*   SUM(SPH_BUF_DOTS), SUM(SPH_BUF_VSIG), gravity, SUM(SPH_BUF_GRAV),     */
+/*   finish, kick.                                                         */
+/* Each summed buffer holds a rank's own contributions and zeros elsewhere,*/
+/* so the sums are exact and every rank continues with identical state.    */
+/* The adjoint and CUDA-graph replay run on unsharded contexts only.       */
+/* ---------------------------------------------------------------------- */
+enum { SPH_BUF_EXCHANGE = 0, SPH_BUF_DOTS = 1, SPH_BUF_VSIG = 2, SPH_BUF_GRAV = 3 };
+/* [lo, hi) of [0, count) owned by shard rank of world (host only) */
+int cudasph_shard_range(long long count, int rank, int world, long long *lo, long long *hi);
+int cudasph_set_shard(sph_ctx *ctx, int rank, int world);
+/* rank, world and the context's leaves [leaf0, leaf1) (any pointer may be NULL) */
+int cudasph_get_shard(sph_ctx *ctx, int *rank, int *world, int *leaf0, int *leaf1);
+/* own h, rho, div, curl, omega, psi, n_ngb into the exchange buffer (zeros elsewhere) */
+int cudasph_shard_pack(sph_ctx *ctx);
+/* the summed exchange buffer back into the state of every particle */
+int cudasph_shard_unpack(sph_ctx *ctx);
+/* device address and length (doubles) of a buffer of the current state */
+int cudasph_device_buffer(sph_ctx *ctx, int which, void **ptr, long long *doubles);
+/* the context's CUDA stream (cudaStream_t) */
+int cudasph_get_stream(sph_ctx *ctx, void **stream);
 
 /* ---------------------------------------------------------------------- */
 /* discrete adjoint of one step (no counterpart in the reference; the      */
