@@ -303,18 +303,21 @@ __global__ void __launch_bounds__(kGA) k_adj_grav_f32(int n, const double4 *__re
 // with their FP32 j-side sums; per two pairs 31 packed FP32 instructions and
 // 2 MUFU.rsq (3 sub, 3 FMA for s^2, 3 mul for s^-2, s^-3 and -3 s^-2, 6 for
 // w, 3 for d.w, 1 for the scale, 3 FMA for w - c d, 3 mul by s^-3, 3 + 3 adds
-// into the i- and j-side sums).
+// into the i- and j-side sums).  Equal masses (the forward step's device
+// flag): w = m (gbar_j - gbar_i), 3 sub instead of 6, the mass applied to the
+// FP64 partial sums; padding sources sit 1e18 away so that s^-3 underflows
+// to 0 (the same form as the forward symmetric kernels).
 constexpr int kAdjWarps = 4;
 constexpr int kAdjRP = 4;
 constexpr int kAdjTile = kAdjWarps * 64 * kAdjRP;  // 1024
 
-__global__ void __launch_bounds__(kAdjWarps * 32) k_adj_grav_sym_f32(int n, int nt, const double4 *__restrict__ src,
-                                                                    const double4 *__restrict__ ab,
-                                                                    double4 *__restrict__ xb, float eps2, double G) {
-  __shared__ float red[2][kAdjWarps][3][32];
-  __shared__ double iacc[2 * kAdjRP * 3][kAdjWarps * 32];  // [i-slot * 3 + component][thread]
+template <bool UNI>
+__device__ __forceinline__ void adj_sym_f32_item(long long item, int n, int nt, const double4 *__restrict__ src,
+                                                 const double4 *__restrict__ ab, double4 *__restrict__ xb,
+                                                 float eps2, double G, float (&red)[2][kAdjWarps][3][32],
+                                                 double (&iacc)[2 * kAdjRP * 3][kAdjWarps * 32]) {
   int b, t_lo, t_hi;
-  sym_item(blockIdx.x, nt, b, t_lo, t_hi);
+  sym_item(item, nt, b, t_lo, t_hi);
   const int j_lo = t_lo * kAdjTile, j_hi = min(t_hi * kAdjTile, n);
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nxt = (l + 1) & 31;
   const int i0 = b * kAdjTile;
@@ -340,10 +343,11 @@ __global__ void __launch_bounds__(kAdjWarps * 32) k_adj_grav_sym_f32(int n, int 
     gx[p] = pk2(u[0], u[1]); gy[p] = pk2(v[0], v[1]); gz[p] = pk2(q[0], q[1]);
   }
   const f32x2 e2 = pk2(eps2, eps2), m3 = pk2(-3.f, -3.f);
+  const double gm = UNI ? G * src[0].w : G;  // UNI: the common mass joins G
   int k = 0;
   for (int jb = j_lo; jb < j_hi; jb += 32, k ^= 1) {
-    float xj = 0.f, yj = 0.f, zj = 0.f, mj = 0.f, gjx = 0.f, gjy = 0.f, gjz = 0.f;
-    if (jb + l < j_hi) {  // padding sources: massless, no gbar, at the anchor
+    float xj = UNI ? 1e18f : 0.f, yj = xj, zj = xj, mj = 0.f, gjx = 0.f, gjy = 0.f, gjz = 0.f;
+    if (jb + l < j_hi) {  // padding sources: massless, no gbar, at the anchor (UNI: far away)
       const double4 s = src[jb + l], g = ab[jb + l];
       xj = (float)(s.x - anc.x); yj = (float)(s.y - anc.y); zj = (float)(s.z - anc.z); mj = (float)s.w;
       gjx = (float)g.x; gjy = (float)g.y; gjz = (float)g.z;
@@ -368,10 +372,10 @@ __global__ void __launch_bounds__(kAdjWarps * 32) k_adj_grav_sym_f32(int n, int 
         const f32x2 inv = pk2(rsqrt_f32(r2a), rsqrt_f32(r2b));
         const f32x2 inv2 = mul2(inv, inv);
         const f32x2 inv3 = mul2(inv2, inv), nc3 = mul2(inv2, m3);
-        // w = m_i gbar_j - m_j gbar_i
-        const f32x2 wx = fma2(mi[p], GX, mul2(NMJ, gx[p]));
-        const f32x2 wy = fma2(mi[p], GY, mul2(NMJ, gy[p]));
-        const f32x2 wz = fma2(mi[p], GZ, mul2(NMJ, gz[p]));
+        // w = m_i gbar_j - m_j gbar_i (UNI: gbar_j - gbar_i, the mass applied later)
+        const f32x2 wx = UNI ? sub2(GX, gx[p]) : fma2(mi[p], GX, mul2(NMJ, gx[p]));
+        const f32x2 wy = UNI ? sub2(GY, gy[p]) : fma2(mi[p], GY, mul2(NMJ, gy[p]));
+        const f32x2 wz = UNI ? sub2(GZ, gz[p]) : fma2(mi[p], GZ, mul2(NMJ, gz[p]));
         const f32x2 nc = mul2(nc3, fma2(dz, wz, fma2(dy, wy, mul2(dx, wx))));  // -3 (d.w) / s^2
         const f32x2 vx = mul2(inv3, fma2(nc, dx, wx));
         const f32x2 vy = mul2(inv3, fma2(nc, dy, wy));
@@ -418,7 +422,7 @@ __global__ void __launch_bounds__(kAdjWarps * 32) k_adj_grav_sym_f32(int n, int 
       double sum = 0.0;
 #pragma unroll
       for (int v = 0; v < kAdjWarps; v++) sum += (double)red[k][v][c][ll];
-      if (jb + ll < j_hi) atomicAdd(&reinterpret_cast<double *>(xb + jb + ll)[c], G * sum);
+      if (jb + ll < j_hi) atomicAdd(&reinterpret_cast<double *>(xb + jb + ll)[c], gm * sum);
     }
   }
 #pragma unroll
@@ -427,23 +431,37 @@ __global__ void __launch_bounds__(kAdjWarps * 32) k_adj_grav_sym_f32(int n, int 
     if (i < n) {
       double *o = reinterpret_cast<double *>(xb + i);
 #pragma unroll
-      for (int c = 0; c < 3; c++) atomicAdd(o + c, G * iacc[r * 3 + c][threadIdx.x]);
+      for (int c = 0; c < 3; c++) atomicAdd(o + c, gm * iacc[r * 3 + c][threadIdx.x]);
     }
   }
 }
 
+// mass_mixed: the forward step's device word, 0 when all masses are equal
+__global__ void __launch_bounds__(kAdjWarps * 32) k_adj_grav_sym_f32(int n, int nt, const double4 *__restrict__ src,
+                                                                    const double4 *__restrict__ ab,
+                                                                    double4 *__restrict__ xb, float eps2, double G,
+                                                                    const int *__restrict__ mass_mixed) {
+  __shared__ float red[2][kAdjWarps][3][32];
+  __shared__ double iacc[2 * kAdjRP * 3][kAdjWarps * 32];  // [i-slot * 3 + component][thread]
+  if (mass_mixed != nullptr && __ldg(mass_mixed) == 0)
+    adj_sym_f32_item<true>(blockIdx.x, n, nt, src, ab, xb, eps2, G, red, iacc);
+  else
+    adj_sym_f32_item<false>(blockIdx.x, n, nt, src, ab, xb, eps2, G, red, iacc);
+}
+
 // Symmetric FP64 form: absolute coordinates, kAdj64R i-particles per lane
-// with their sums in registers.
+// with their sums in registers; equal masses as in the mixed form (padding
+// sources 1e150 away).
 constexpr int kAdj64Warps = 4;
 constexpr int kAdj64R = 8;
 static_assert(kAdj64Warps * 32 * kAdj64R == kAdjTile, "the FP64 form shares the tile layout");
 
-__global__ void __launch_bounds__(kAdj64Warps * 32) k_adj_grav_sym_f64(int n, int nt, const double4 *__restrict__ src,
-                                                                      const double4 *__restrict__ ab,
-                                                                      double4 *__restrict__ xb, double eps2, double G) {
-  __shared__ double red[2][kAdj64Warps][3][32];
+template <bool UNI>
+__device__ __forceinline__ void adj_sym_f64_item(long long item, int n, int nt, const double4 *__restrict__ src,
+                                                 const double4 *__restrict__ ab, double4 *__restrict__ xb,
+                                                 double eps2, double G, double (&red)[2][kAdj64Warps][3][32]) {
   int b, t_lo, t_hi;
-  sym_item(blockIdx.x, nt, b, t_lo, t_hi);
+  sym_item(item, nt, b, t_lo, t_hi);
   const int j_lo = t_lo * kAdjTile, j_hi = min(t_hi * kAdjTile, n);
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nxt = (l + 1) & 31;
   const int ib = b * kAdjTile + w * 32 * kAdj64R + l;
@@ -460,10 +478,12 @@ __global__ void __launch_bounds__(kAdj64Warps * 32) k_adj_grav_sym_f64(int n, in
     gx[r] = g.x; gy[r] = g.y; gz[r] = g.z;
     rx[r] = ry[r] = rz[r] = 0.0;
   }
+  const double gm = UNI ? G * src[0].w : G;  // UNI: the common mass joins G
   int k = 0;
   for (int jb = j_lo; jb < j_hi; jb += 32, k ^= 1) {
     const bool in = jb + l < j_hi;
-    const double4 s = in ? src[jb + l] : make_double4(far.x, far.y, far.z, 0.0);
+    const double4 s = in ? src[jb + l] : (UNI ? make_double4(1e150, 1e150, 1e150, 0.0)
+                                              : make_double4(far.x, far.y, far.z, 0.0));
     const double4 g = in ? ab[jb + l] : make_double4(0.0, 0.0, 0.0, 0.0);
     double xj = s.x, yj = s.y, zj = s.z, mj = s.w, gjx = g.x, gjy = g.y, gjz = g.z;
     double ajx = 0.0, ajy = 0.0, ajz = 0.0;
@@ -475,7 +495,9 @@ __global__ void __launch_bounds__(kAdj64Warps * 32) k_adj_grav_sym_f64(int n, in
         const double s2 = fma(dz, dz, fma(dy, dy, fma(dx, dx, eps2)));
         const double inv = rsqrt_f64(s2);
         const double inv2 = inv * inv, inv3 = inv2 * inv;
-        const double wx = mi[r] * gjx - mj * gx[r], wy = mi[r] * gjy - mj * gy[r], wz = mi[r] * gjz - mj * gz[r];
+        const double wx = UNI ? gjx - gx[r] : mi[r] * gjx - mj * gx[r];
+        const double wy = UNI ? gjy - gy[r] : mi[r] * gjy - mj * gy[r];
+        const double wz = UNI ? gjz - gz[r] : mi[r] * gjz - mj * gz[r];
         const double c = 3.0 * inv2 * (dx * wx + dy * wy + dz * wz);
         const double vx = inv3 * (wx - c * dx), vy = inv3 * (wy - c * dy), vz = inv3 * (wz - c * dz);
         rx[r] += vx; ry[r] += vy; rz[r] += vz;
@@ -501,7 +523,7 @@ __global__ void __launch_bounds__(kAdj64Warps * 32) k_adj_grav_sym_f64(int n, in
       double sum = 0.0;
 #pragma unroll
       for (int v = 0; v < kAdj64Warps; v++) sum += red[k][v][c][ll];
-      if (jb + ll < j_hi) atomicAdd(&reinterpret_cast<double *>(xb + jb + ll)[c], G * sum);
+      if (jb + ll < j_hi) atomicAdd(&reinterpret_cast<double *>(xb + jb + ll)[c], gm * sum);
     }
   }
 #pragma unroll
@@ -509,11 +531,22 @@ __global__ void __launch_bounds__(kAdj64Warps * 32) k_adj_grav_sym_f64(int n, in
     const int i = ib + r * 32;
     if (i < n) {
       double *o = reinterpret_cast<double *>(xb + i);
-      atomicAdd(o + 0, G * rx[r]);
-      atomicAdd(o + 1, G * ry[r]);
-      atomicAdd(o + 2, G * rz[r]);
+      atomicAdd(o + 0, gm * rx[r]);
+      atomicAdd(o + 1, gm * ry[r]);
+      atomicAdd(o + 2, gm * rz[r]);
     }
   }
+}
+
+__global__ void __launch_bounds__(kAdj64Warps * 32) k_adj_grav_sym_f64(int n, int nt, const double4 *__restrict__ src,
+                                                                      const double4 *__restrict__ ab,
+                                                                      double4 *__restrict__ xb, double eps2, double G,
+                                                                      const int *__restrict__ mass_mixed) {
+  __shared__ double red[2][kAdj64Warps][3][32];
+  if (mass_mixed != nullptr && __ldg(mass_mixed) == 0)
+    adj_sym_f64_item<true>(blockIdx.x, n, nt, src, ab, xb, eps2, G, red);
+  else
+    adj_sym_f64_item<false>(blockIdx.x, n, nt, src, ab, xb, eps2, G, red);
 }
 
 // -- 6. hydro VJP (warp per leaf, lane per particle, lists of find_ngb) ------
@@ -982,7 +1015,8 @@ __global__ void k_adj_predict_final(AdjArgs a, int nb) {
 int adjoint_part_doubles(int n) { return 3 * ((n + kAT - 1) / kAT) + 8; }
 
 // The whole reverse sweep; src = packed gravity sources {x1, m} of the step.
-int launch_adjoint(AdjArgs a, const double4 *src, double eps, double G, int precision, cudaStream_t st) {
+int launch_adjoint(AdjArgs a, const double4 *src, const int *mass_mixed, double eps, double G, int precision,
+                   cudaStream_t st) {
   const int n = a.n;
   const int nb = (n + kAT - 1) / kAT;
   const int warps_blocks = (a.nleaf * 32 + 127) / 128;
@@ -1006,10 +1040,11 @@ int launch_adjoint(AdjArgs a, const double4 *src, double eps, double G, int prec
     launches++;
     if (nt >= 2) {
       if (precision == SPH_PREC_FP64)
-        k_adj_grav_sym_f64<<<(unsigned)sym_S(nt - 1), kAdj64Warps * 32, 0, st>>>(n, nt, src, a.ab, a.xb, eps * eps, G);
+        k_adj_grav_sym_f64<<<(unsigned)sym_S(nt - 1), kAdj64Warps * 32, 0, st>>>(n, nt, src, a.ab, a.xb, eps * eps, G,
+                                                                                  mass_mixed);
       else
         k_adj_grav_sym_f32<<<(unsigned)sym_S(nt - 1), kAdjWarps * 32, 0, st>>>(n, nt, src, a.ab, a.xb,
-                                                                            (float)(eps * eps), G);
+                                                                            (float)(eps * eps), G, mass_mixed);
       launches++;
     }
   }

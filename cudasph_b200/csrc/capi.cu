@@ -50,7 +50,8 @@ int launch_field_io(int n, double *arr, int stride, int comp, const int *id, dou
                     cudaStream_t st);
 int launch_iota(int n, int *id, cudaStream_t st);
 int adjoint_part_doubles(int n);
-int launch_adjoint(AdjArgs a, const double4 *src, double eps, double G, int precision, cudaStream_t st);
+int launch_adjoint(AdjArgs a, const double4 *src, const int *mass_mixed, double eps, double G, int precision,
+                   cudaStream_t st);
 }  // namespace sph
 
 using namespace sph;
@@ -971,7 +972,7 @@ extern "C" int cudasph_adjoint(sph_ctx *c) {
   a.alpha = c->p.av_alpha; a.beta = c->p.av_beta; a.gamma = c->p.gamma; a.cn1 = c->p.cn1; a.cn2 = c->p.cn2;
   a.eos_mode = c->p.eos_mode; a.use_psi = use_psi(c->p);
   PhaseScope ps(c, SPH_PH_ADJOINT);
-  c->launches += launch_adjoint(a, c->gsrc, c->p.eps, c->p.G, c->p.precision, c->st);
+  c->launches += launch_adjoint(a, c->gsrc, c->mass_mixed, c->p.eps, c->p.G, c->p.precision, c->st);
   // the density injection is per step
   SPH_CUDA_TRY(cudaMemsetAsync(c->rho_ext, 0, sizeof(double) * c->n, c->st));
   SPH_CUDA_TRY(cudaGetLastError());
