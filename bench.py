@@ -198,9 +198,16 @@ SPH_BYTES = {
 }
 
 
+# bytes of neighbour records each pair gathers (served by L1/L2): density
+# reads pos + vel of j, hydro pos + vel + hyd + dd of j
+SPH_GATHER = {"density": 64, "hydro": 128}
+
+
 def sph_bandwidth(ph, steps, n, nbar):
     """Achieved HBM bandwidth of the bandwidth-bound phases (device time per
-    step from the CUDA-event phase timers) against the measured copy peak."""
+    step from the CUDA-event phase timers) against the measured copy peak,
+    and the rate at which the pair loops gather neighbour records from L1/L2
+    (no measured L2 peak on this pool: reported as a rate only)."""
     peak, src = measured_hbm_gbs()
     out = {"peak_gbs": peak, "peak_source": src, "mean_neighbours": nbar}
     for k, f in SPH_BYTES.items():
@@ -210,6 +217,8 @@ def sph_bandwidth(ph, steps, n, nbar):
         b = f(nbar) * n
         out[k] = {"ms": round(ms, 4), "bytes_per_particle": round(f(nbar), 1), "gbs": round(b / (ms * 1e-3) / 1e9, 1),
                   "frac": round(b / (ms * 1e-3) / 1e9 / peak, 4)}
+        if k in SPH_GATHER:
+            out[k]["gather_gbs"] = round(SPH_GATHER[k] * nbar * n / (ms * 1e-3) / 1e9, 1)
     return out
 
 

@@ -22,7 +22,12 @@ namespace sph {
 constexpr int kWarpsPerBlock = 4;
 constexpr unsigned kFull = 0xffffffffu;
 
+struct LaneBox {
+  float lo[3], hi[3];
+};
+
 struct WarpSmem {
+  LaneBox lbox[kLeaf];  // the lanes' query boxes of the current walk
   int stack[kStack];
   double sx[kLeaf], sy[kLeaf], sz[kLeaf];
   float4 sf[kLeaf];  // anchor-relative FP32 copies for the pre-filter
@@ -96,11 +101,9 @@ __device__ __forceinline__ void warp_query_box(bool on, double x, double y, doub
 // This lane's own query box [x - r, x + r], widened and rounded outward like
 // warp_query_box.  A leaf whose box misses it holds no j with d2 < r^2 for
 // this lane (both boxes contain everything they should), so the lane skips
-// the leaf's candidates: the sets are unchanged, the work drops by half.
-struct LaneBox {
-  float lo[3], hi[3];
-};
-
+// the leaf's candidates, and the walk descends only into nodes whose box
+// meets the box of at least one active lane (not merely the union of the
+// lanes' boxes): the sets are unchanged, the work drops by more than half.
 __device__ __forceinline__ LaneBox lane_query_box(double x, double y, double z, double r) {
   const double m0 = (fabs(x) + r) * 1e-15, m1 = (fabs(y) + r) * 1e-15, m2 = (fabs(z) + r) * 1e-15;
   LaneBox b;
@@ -114,11 +117,23 @@ __device__ __forceinline__ bool lane_box_hits(const LaneBox &q, const float *bl,
          (bh[2] >= q.lo[2]);
 }
 
-// Visit, in ascending order, every leaf whose box overlaps [ql, qh].  All
-// lanes call visit(leaf, lo, hi) together, lo / hi = the leaf's box (float,
-// rounded outward).  Returns false on stack overflow.
+// publish this lane's query box to the warp; returns the mask of active lanes
+__device__ __forceinline__ unsigned share_lane_boxes(WarpSmem &sm, const LaneBox &lb, bool on) {
+  __syncwarp();
+  sm.lbox[lane_id()] = lb;
+  const unsigned m = __ballot_sync(kFull, on);
+  __syncwarp();
+  return m;
+}
+
+// Visit, in ascending order, every leaf whose box overlaps [ql, qh] (the
+// union of the lanes' query boxes) and the query box of at least one lane of
+// `onmask` (boxes in lbs).  All lanes call visit(leaf, lo, hi) together,
+// lo / hi = the leaf's box (float, rounded outward).  Returns false on stack
+// overflow.
 template <class Visit>
-__device__ bool walk_leaves(const TreeView &t, const float *ql, const float *qh, int *stack, Visit &&visit) {
+__device__ bool walk_leaves(const TreeView &t, const float *ql, const float *qh, const LaneBox *lbs,
+                            unsigned onmask, int *stack, Visit &&visit) {
   const unsigned lane = lane_id();
   const int top = t.levels - 1;
   if (top == 0) {
@@ -142,6 +157,18 @@ __device__ bool walk_leaves(const TreeView &t, const float *ql, const float *qh,
       l = __ldg(&t.lo[t.base[cl] + child]);
       h = __ldg(&t.hi[t.base[cl] + child]);
       hit = (l.x <= qh[0]) & (h.x >= ql[0]) & (l.y <= qh[1]) & (h.y >= ql[1]) & (l.z <= qh[2]) & (h.z >= ql[2]);
+    }
+    if (hit) {  // ... and the box of some active lane
+      bool any = false;
+      unsigned mm = onmask;
+      while (mm && !any) {
+        const int L = __ffs(mm) - 1;
+        mm &= mm - 1;
+        const LaneBox q = lbs[L];
+        any = (l.x <= q.hi[0]) & (h.x >= q.lo[0]) & (l.y <= q.hi[1]) & (h.y >= q.lo[1]) & (l.z <= q.hi[2]) &
+              (h.z >= q.lo[2]);
+      }
+      hit = any;
     }
     unsigned m = __ballot_sync(kFull, hit);
     if (cl == 0) {
@@ -262,7 +289,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 6) k_solve_range(SolveArg
       const float thr = prefilter_threshold(pf, r);
       int c = 0;
       const LaneBox lb = lane_query_box(xi, yi, zi, r);
-      stack_ok &= walk_leaves(a.t, ql, qh, sm.stack, [&](int lj, const float *bl, const float *bh) {
+      const unsigned onmask = share_lane_boxes(sm, lb, on);
+      stack_ok &= walk_leaves(a.t, ql, qh, sm.lbox, onmask, sm.stack, [&](int lj, const float *bl, const float *bh) {
         stage_leaf(a.pos, n, lj, sm, pf);
         const int cntj = min(kLeaf, n - lj * kLeaf);
         if (on && lane_box_hits(lb, bl, bh)) {
@@ -445,7 +473,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_find_ngb(FindArgs a) {
   bool ok = true;
   if (__any_sync(kFull, on)) {
     const LaneBox lb = lane_query_box(xi, yi, zi, w);
-    ok = walk_leaves(a.t, ql, qh, sm.stack, [&](int lj, const float *bl, const float *bh) {
+    const unsigned onmask = share_lane_boxes(sm, lb, on);
+    ok = walk_leaves(a.t, ql, qh, sm.lbox, onmask, sm.stack, [&](int lj, const float *bl, const float *bh) {
       stage_leaf(a.pos, n, lj, sm, pf);
       const int m = min(kLeaf, n - lj * kLeaf);
       if (on && lane_box_hits(lb, bl, bh)) {
