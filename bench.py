@@ -293,6 +293,36 @@ def adjoint_cost(steps=5, warmup=3, headline_n=None):
     return out
 
 
+def tree_gravity(ic, thetas=(0.3, 0.5), reps=3, params=None):
+    """The opt-in Barnes-Hut gravity (grav_mode = tree, quadrupoles) on the
+    same state as the headline: CUDA-event time of the gravity phase (node
+    moments + walk) per opening angle and its RMS force error against the
+    direct mixed-precision sum (itself within 4e-8 of FP64 on this workload).
+    The direct sum stays the headline path."""
+    from cudasph_b200.simulation import Simulation, make_params
+    params = params or WORKLOAD_PARAMS
+    d = Simulation(ic, make_params(**dict(params, precision=1)))
+    d.CUDA_gravity()
+    gd = np.stack([d.get(k) for k in ("gx", "gy", "gz")], 1)
+    d.close()
+    out = {}
+    for th in thetas:
+        s = Simulation(ic, make_params(**dict(params, precision=1, grav_mode=1, theta=th)))
+        s.CUDA_gravity()  # sort + tree
+        s.synchronize()
+        s.reset_counters()
+        s.set_profiling(True)
+        for _ in range(reps):
+            s.CUDA_gravity()
+        ph = s.phase_times()
+        s.set_profiling(False)
+        g = np.stack([s.get(k) for k in ("gx", "gy", "gz")], 1)
+        out[f"theta_{th}"] = {"ms": ph["gravity"][0] / reps, "rms_force_rel_vs_direct": rms_rel(g, gd),
+                              "flags": s.device_status()}
+        s.close()
+    return out
+
+
 def energy_drift(n, steps):
     """Energy conservation over `steps` steps of the bench workload at N = n:
     the mixed form and the FP64 form run side by side from the same initial
@@ -364,6 +394,8 @@ def large_run(n=LARGE_N, steps=5, n_sub=262144):
     res["stats_last_step"] = {k: v for k, v in sim.system_statistics().items() if k in ("E", "dt", "ngb_mean")}
     res["device_flags"] = sim.device_status()
     sim.close()
+    # the opt-in tree gravity on the initial state, against the direct sum
+    res["tree_gravity_initial_state"] = tree_gravity(ic, params=LARGE_PARAMS)
 
     rng = np.random.default_rng(12345 + 5)
     idx = np.sort(rng.choice(n, n_sub, replace=False))
@@ -521,6 +553,10 @@ def run_ours(args, rank, world):
                        "gravity_ms": g64ms, "gravity_frac_of_fp64_peak": flops / (g64ms * 1e-3) / peak64}
         out["mixed_over_fp64"] = ms64 / ms_step
         out["errors"] = errors
+
+    # --- the opt-in tree gravity on the same state -------------------------------------
+    if args.tree:
+        out["tree_gravity"] = tree_gravity(ic)
 
     # --- adjoint / forward cost (the differentiation form) --------------------------
     if args.adjoint:
@@ -708,6 +744,8 @@ def main():
     ap.add_argument("--cpu-grav-targets", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false")
+    ap.add_argument("--no-tree", dest="tree", action="store_false",
+                    help="skip the tree-gravity measurement (opt-in Barnes-Hut mode)")
     ap.add_argument("--sharded", action="store_true",
                     help="run the sharded multi-GPU path also at N = 1 (a one-rank NCCL process group)")
     ap.add_argument("--drift-steps", type=int, default=0,

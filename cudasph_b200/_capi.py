@@ -41,7 +41,7 @@ class Params(C.Structure):
         ("av_alpha", C.c_double), ("av_beta", C.c_double), ("gamma", C.c_double), ("eos_mode", C.c_int),
         ("soft_mode", C.c_int), ("eps", C.c_double), ("use_psi", C.c_int), ("cn1", C.c_double),
         ("cn2", C.c_double), ("G", C.c_double), ("precision", C.c_int), ("ngb_cap", C.c_int),
-        ("sort_every", C.c_int), ("mixed_sph", C.c_int),
+        ("sort_every", C.c_int), ("mixed_sph", C.c_int), ("grav_mode", C.c_int), ("theta", C.c_double),
     ]
 
 

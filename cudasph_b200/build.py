@@ -26,7 +26,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relax
 # no FMA contraction: results reproducible against an FP64 CPU evaluation
 NO_FMAD = {"neighbours.cu", "hydro.cu"}
 SOURCES = ["sort.cu", "tree.cu", "neighbours.cu", "hydro.cu", "hydro_mixed.cu", "gravity.cu", "integrate.cu",
-           "capi.cu", "legacy.cu", "peak.cu", "adjoint.cu"]
+           "capi.cu", "legacy.cu", "peak.cu", "adjoint.cu", "treegrav.cu"]
 
 
 def nvcc() -> str:

@@ -30,6 +30,8 @@ int launch_density_mixed(const HydroArgs &a, cudaStream_t st);
 int launch_hydro_mixed(const HydroArgs &a, cudaStream_t st);
 int launch_gravity(int n, const double4 *src, const double *h2src, double4 *out, int soft_mode, double eps, double G,
                    int precision, const int *mass_mixed, int rank, int world, cudaStream_t st);
+int launch_tree_gravity(const TreeView &t, const double4 *src, double4 *cm, double4 *q0, double4 *q1, double4 *out,
+                        unsigned *flags, double eps, double theta, double G, int rank, int world, cudaStream_t st);
 int launch_shard_pack(int n, int s0, int s1, const double4 *pos, const double4 *hyd, const double4 *dd,
                       const int *n_ngb, double4 *xbuf, cudaStream_t st);
 int launch_shard_unpack(int n, const double4 *xbuf, double4 *pos, double4 *hyd, double4 *dd, int *n_ngb,
@@ -82,6 +84,7 @@ struct sph_ctx {
   double *dcache = nullptr;  // candidate squared distances of the h solve, layout of list
   TreeView tree;
   float4 *tlo = nullptr, *thi = nullptr;
+  double4 *tcm = nullptr, *tq0 = nullptr, *tq1 = nullptr;  // tree-gravity node moments
   uint64_t *keys = nullptr;
   uint32_t *vals = nullptr;
   void *sort_scratch = nullptr;
@@ -185,6 +188,9 @@ int check_params(const sph_params *p) {
   if (p->precision != SPH_PREC_FP64 && p->precision != SPH_PREC_MIXED) return SPH_ERR_ARG;
   if (p->ngb_cap < 0 || p->sort_every < 0 || p->mixed_sph < 0 || p->mixed_sph > 3) return SPH_ERR_ARG;
   if (!(p->gamma > 1)) return SPH_ERR_ARG;
+  if (p->grav_mode != SPH_GRAV_DIRECT && p->grav_mode != SPH_GRAV_TREE) return SPH_ERR_ARG;
+  if (p->grav_mode == SPH_GRAV_TREE && (p->soft_mode != SPH_SOFT_PLUMMER || !(p->theta >= 0) || !(p->theta < 1)))
+    return SPH_ERR_ARG;
   return SPH_OK;
 }
 
@@ -256,6 +262,8 @@ extern "C" sph_params cudasph_default_params(void) {
   p.ngb_cap = 0;
   p.sort_every = 1;
   p.mixed_sph = 0;
+  p.grav_mode = SPH_GRAV_DIRECT;
+  p.theta = 0.5;
   return p;
 }
 
@@ -269,7 +277,7 @@ extern "C" int cudasph_destroy(sph_ctx *c) {
     cudaFree(F.vsig); cudaFree(F.id);
   }
   cudaFree(c->old); cudaFree(c->n_ngb); cudaFree(c->nevals); cudaFree(c->list); cudaFree(c->dcache);
-  cudaFree(c->tlo); cudaFree(c->thi); cudaFree(c->keys); cudaFree(c->vals); cudaFree(c->sort_scratch);
+  cudaFree(c->tlo); cudaFree(c->thi); cudaFree(c->tcm); cudaFree(c->tq0); cudaFree(c->tq1); cudaFree(c->keys); cudaFree(c->vals); cudaFree(c->sort_scratch);
   cudaFree(c->bbox_part); cudaFree(c->box4); cudaFree(c->gsrc); cudaFree(c->gh2); cudaFree(c->mass_mixed); cudaFree(c->xbuf); cudaFree(c->flags);
   cudaFree(c->sc); cudaFree(c->fin_part); cudaFree(c->flat); cudaFree(c->slot_of);
   cudaFree(c->pre_acc); cudaFree(c->xb); cudaFree(c->vb); cudaFree(c->ab); cudaFree(c->vpb); cudaFree(c->vpup);
@@ -324,6 +332,9 @@ extern "C" int cudasph_create(const sph_params *params, int n, int device, sph_c
   TRY_ALLOC(dalloc(&c->nevals, n));
   TRY_ALLOC(dalloc(&c->tlo, nodes));
   TRY_ALLOC(dalloc(&c->thi, nodes));
+  TRY_ALLOC(dalloc(&c->tcm, nodes));
+  TRY_ALLOC(dalloc(&c->tq0, nodes));
+  TRY_ALLOC(dalloc(&c->tq1, nodes));
   TRY_ALLOC(dalloc(&c->keys, n));
   TRY_ALLOC(dalloc(&c->vals, n));
   TRY_ALLOC(dalloc((char **)&c->sort_scratch, radix_scratch_bytes(n)));
@@ -657,9 +668,20 @@ extern "C" int cudasph_sph_accelerations(sph_ctx *c) {
 
 extern "C" int cudasph_gravity(sph_ctx *c) {
   if (!c) return SPH_ERR_ARG;
+  if (c->p.grav_mode == SPH_GRAV_TREE && !c->tree_ok) {
+    int rc = cudasph_build_tree(c);
+    if (rc) return rc;
+  }
   SPH_CUDA_TRY(cudaSetDevice(c->device));
   PhaseScope ps(c, SPH_PH_GRAVITY);
   Fields &F = c->f[c->cur];
+  if (c->p.grav_mode == SPH_GRAV_TREE) {
+    LAUNCHED(launch_pack_sources(c->n, F.pos, F.vel, c->gsrc, c->gh2, c->mass_mixed, c->st));
+    LAUNCHED(launch_tree_gravity(c->tree, c->gsrc, c->tcm, c->tq0, c->tq1, F.grav, c->flags, c->p.eps, c->p.theta,
+                                 c->p.G, c->rank, c->world, c->st));
+    SPH_CUDA_TRY(cudaGetLastError());
+    return SPH_OK;
+  }
   LAUNCHED(launch_pack_sources(c->n, F.pos, F.vel, c->gsrc, c->gh2, c->mass_mixed, c->st));
   LAUNCHED(launch_gravity(c->n, c->gsrc, c->gh2, F.grav, c->p.soft_mode, c->p.eps, c->p.G, c->p.precision,
                           c->mass_mixed, c->rank, c->world, c->st));
@@ -951,8 +973,8 @@ extern "C" int cudasph_adjoint(sph_ctx *c) {
     sph_internal_set_error("cudasph_adjoint: the last step was not taken with cudasph_set_keep(ctx, 1)");
     return SPH_ERR_STATE;
   }
-  if (c->p.soft_mode != SPH_SOFT_PLUMMER) {
-    sph_internal_set_error("cudasph_adjoint: implemented for Plummer softening");
+  if (c->p.soft_mode != SPH_SOFT_PLUMMER || c->p.grav_mode != SPH_GRAV_DIRECT) {
+    sph_internal_set_error("cudasph_adjoint: implemented for direct Plummer gravity");
     return SPH_ERR_ARG;
   }
   SPH_CUDA_TRY(cudaSetDevice(c->device));

@@ -54,6 +54,7 @@ typedef enum {
 typedef enum { SPH_EOS_IDEAL = 0, SPH_EOS_GAS_RADIATION = 1 } sph_eos_mode;
 typedef enum { SPH_SOFT_SPLINE = 0, SPH_SOFT_PLUMMER = 1 } sph_soft_mode;
 typedef enum { SPH_PREC_FP64 = 0, SPH_PREC_MIXED = 1 } sph_precision;
+typedef enum { SPH_GRAV_DIRECT = 0, SPH_GRAV_TREE = 1 } sph_grav_mode;
 
 typedef struct {
   double n_target;   /* smoothed neighbour number; DESIRED_NGB, dev_solve_range.cu:14 */
@@ -78,6 +79,11 @@ typedef struct {
                         1M-particle step, while FP32 ones raise the RMS total-force error of a
                         star near hydrostatic equilibrium (hydro and gravity nearly cancel)
                         from 4.9e-7 to 2.2e-5 */
+  int grav_mode;     /* sph_grav_mode: direct N^2 sum (the reference's sph_grav_kernel.cu, default)
+                        or the Barnes-Hut tree with quadrupoles (no counterpart in the reference;
+                        Plummer softening only; force error set by theta) */
+  double theta;      /* tree opening angle: a node of radius b is accepted when b < theta * its
+                        distance to the target group's box (default 0.5) */
 } sph_params;
 
 /* particle fields, addressed in the caller's ORIGINAL particle order */
