@@ -429,6 +429,89 @@ def large_run(n=LARGE_N, steps=5, n_sub=262144):
     return res
 
 
+C2_N = 262144
+C2_PARAMS = dict(n_target=64.0, eos_mode=1, soft_mode=1, eps=0.005)
+
+
+def c2_run(n=C2_N, steps=50, n_grav_targets=512):
+    """The plain FP64 workload at N = 262,144 (n=1.5 polytrope with a seeded
+    5 % perturbation of u, ideal gas + radiation EOS mu = 0.62, N_ngb = 64,
+    Plummer eps = 0.005): `steps` FP64 steps on the GPU (device time per
+    phase, CUDA events; energy change over the run), and the same phases on
+    the CPU on the same initial state, each kernel against its CPU
+    counterpart: the FP64 oracle restatement of the reference loops with the
+    same parameters (OpenMP over all host threads; gravity on a seeded sample
+    of targets extrapolated to n) and the reference's own code built for the
+    host (its compiled-in DESIRED_NGB = 24 and spline softening)."""
+    from cudasph_b200 import ics
+    from cudasph_b200.simulation import Simulation, make_params
+    from oracle import oracle as O
+    ic = ics.polytrope(n, n_poly=1.5, n_ngb=64.0, seed=12345 + 2, u_jitter=0.05, mu=0.62)
+    res = {"workload": f"n=1.5 polytrope, N={n}, u x (1 + U(-0.05, 0.05)), gas+radiation EOS mu=0.62, N_ngb=64, "
+                       f"Plummer eps=0.005, FP64", "steps": steps}
+    # GPU: the first step separately (h solved from the initial guess), then the run
+    sim = Simulation(ic, make_params(precision=0, **C2_PARAMS))
+    sim.reset_counters()
+    sim.set_profiling(True)
+    sim.step()
+    sim.synchronize()
+    first = sim.phase_times()
+    sim.reset_counters()
+    E0 = sim.system_statistics()["E"]
+    sim.step(steps - 1)
+    sim.synchronize()
+    ph = sim.phase_times()
+    sim.set_profiling(False)
+    E1 = sim.system_statistics()["E"]
+    gpu = {k: v[0] / (steps - 1) for k, v in ph.items() if v[1] > 0}
+    res["gpu_ms_per_step"] = {k: round(v, 4) for k, v in gpu.items()}
+    res["gpu_first_step_ms"] = {k: round(v[0], 4) for k, v in first.items() if v[1] > 0}
+    res["energy_change_rel"] = (E1 - E0) / abs(E0)
+    res["device_flags"] = sim.device_status()
+    sim.close()
+    # CPU: the FP64 oracle, phase by phase, on the initial state with the same parameters
+    par = O.make_params(**C2_PARAMS)
+    t = {}
+    t0 = time.perf_counter()
+    rng, _, _ = O.solve_range(ic["x"], ic["y"], ic["z"], ic["range"], par)
+    t["solve_range"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    cnt, off, lst = O.find_ngb(ic["x"], ic["y"], ic["z"], rng)
+    t["find_ngb"] = time.perf_counter() - t0
+    st = dict(ic, range=rng)
+    t0 = time.perf_counter()
+    st.update(O.density(st, off, lst))
+    t["density"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    st["P"] = O.pressure(st["rho"], st["u"], st["mu"], par)
+    t["pressure"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    O.hydro(st, off, lst, par)
+    t["hydro"] = time.perf_counter() - t0
+    tg = np.random.default_rng(0).choice(n, size=n_grav_targets, replace=False).astype(np.int32)
+    t0 = time.perf_counter()
+    O.gravity(ic["x"], ic["y"], ic["z"], ic["m"], rng, par, targets=tg)
+    t["gravity"] = (time.perf_counter() - t0) * n / n_grav_targets
+    # the GPU's h solve writes the lists (find_ngb fused), so compare the pair
+    cpu_ms = {k: 1000.0 * v for k, v in t.items()}
+    gpu_solve = gpu.get("solve_range", 0.0) + gpu.get("find_ngb", 0.0)
+    rows = {"solve_range + find_ngb": (cpu_ms["solve_range"] + cpu_ms["find_ngb"], gpu_solve)}
+    for k in ("density", "pressure", "hydro", "gravity"):
+        rows[k] = (cpu_ms[k], gpu.get(k, 0.0))
+    res["per_kernel_vs_oracle_cpu"] = {
+        k: {"cpu_ms": round(c, 2), "gpu_ms": round(g, 4), "speedup": round(c / g, 1) if g > 0 else None}
+        for k, (c, g) in rows.items()}
+    res["oracle_cpu_threads"] = O.num_threads()
+    res["oracle_cpu_note"] = (f"FP64 oracle on the initial state, same parameters; gravity on {n_grav_targets} "
+                              f"seeded targets x {n} sources, extrapolated")
+    # the reference's own code built for the host, on the same state (its compiled-in parameters)
+    if O.ref_available():
+        r = O.RefPipeline(ic).time_step(n_grav_targets=256)
+        res["reference_cpu_build_s"] = {k: round(v, 3) for k, v in r.items()}
+        res["reference_cpu_threads"] = O.ref().ref_num_threads()
+    return res
+
+
 def cpu_reference_sample(ic, n_grav_targets=256):
     from oracle import oracle as O
     if not O.ref_available():
@@ -750,12 +833,18 @@ def main():
                     help="run the sharded multi-GPU path also at N = 1 (a one-rank NCCL process group)")
     ap.add_argument("--drift-steps", type=int, default=0,
                     help="instead of the bench line, measure energy drift over this many steps (mixed vs FP64)")
+    ap.add_argument("--c2", action="store_true",
+                    help="instead of the bench line, run the N = 262,144 plain FP64 workload (50 steps) with each "
+                         "kernel timed against its CPU counterpart")
     ap.add_argument("--large", action="store_true",
                     help="instead of the bench line, run the N = 4,194,304 cold-sphere workload (5 steps + a subset "
                          "adjoint)")
     args = ap.parse_args()
     if args.large:
         print(json.dumps({"measurement": "large_cold_sphere", **large_run()}), flush=True)
+        return
+    if args.c2:
+        print(json.dumps({"measurement": "fp64_262k_per_kernel", **c2_run()}), flush=True)
         return
     if args.drift_steps > 0:
         print(json.dumps({"measurement": "energy_drift", **energy_drift(args.n, args.drift_steps)}), flush=True)
