@@ -9,6 +9,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "common.cuh"
 
 namespace sph {
@@ -125,11 +127,19 @@ static void drop_graphs(sph_ctx *c);
 
 namespace {
 
+// Every phase is an NVTX range on the host thread (names below; a profiler
+// attached to the process shows the step's structure) and, with profiling
+// on, a pair of CUDA events on the context's stream (cudasph_phase_times).
+const char *const kPhaseNames[SPH_NPHASES] = {"sph:sort",    "sph:predict", "sph:tree",     "sph:solve_range",
+                                              "sph:find_ngb", "sph:density", "sph:pressure", "sph:hydro",
+                                              "sph:gravity", "sph:finish",  "sph:kick",     "sph:adjoint"};
+
 struct PhaseScope {
   sph_ctx *c;
   int ph;
   cudaEvent_t b = nullptr;
   PhaseScope(sph_ctx *c_, int ph_) : c(c_), ph(ph_) {
+    nvtxRangePushA(kPhaseNames[ph]);
     if (!c->profiling) return;
     b = take();
     cudaEventRecord(b, c->st);
@@ -145,6 +155,7 @@ struct PhaseScope {
     return e;
   }
   ~PhaseScope() {
+    nvtxRangePop();
     if (!c->profiling) return;
     cudaEvent_t e = take();
     cudaEventRecord(e, c->st);
