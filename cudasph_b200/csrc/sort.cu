@@ -8,7 +8,6 @@
 // exclusive scan over [digit][block], and a stable scatter in which each
 // warp ranks equal digits with __match_any_sync.  Ties keep their input
 // order, so with values = slot indices the permutation equals a stable sort.
-#include <cub/block/block_scan.cuh>
 #include <cstdio>
 
 #include "common.cuh"
@@ -110,20 +109,45 @@ __global__ void __launch_bounds__(kRadixThreads) k_radix_hist(int n, const uint6
   hist[threadIdx.x * gridDim.x + blockIdx.x] = h[threadIdx.x];
 }
 
-// exclusive scan of m entries in one block of 1024 threads
+// exclusive scan of m entries in one block of 1024 threads: warp w owns the
+// contiguous segment [w * seg, (w + 1) * seg) and walks it in coalesced
+// 32-entry chunks (warp shuffle scan per chunk); a first pass sums the
+// segments, a block scan of the 32 segment sums gives each warp its offset,
+// a second pass writes the prefixes.
 __global__ void __launch_bounds__(1024) k_radix_scan(int m, unsigned *__restrict__ hist) {
-  typedef cub::BlockScan<unsigned, 1024> Scan;
-  __shared__ typename Scan::TempStorage tmp;
-  int per = (m + 1023) / 1024;
-  int beg = threadIdx.x * per, end = min(m, beg + per);
-  unsigned s = 0;
-  for (int i = beg; i < end; i++) s += hist[i];
-  unsigned pre;
-  Scan(tmp).ExclusiveSum(s, pre);
-  for (int i = beg; i < end; i++) {
-    unsigned v = hist[i];
-    hist[i] = pre;
-    pre += v;
+  __shared__ unsigned seg_sum[32];
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  const int seg = (m + 31) / 32;
+  const int beg = w * seg, end = min(m, beg + seg);
+  unsigned tot = 0;
+  for (int i = beg + l; i < end; i += 32) tot += hist[i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+  if (l == 0) seg_sum[w] = tot;
+  __syncthreads();
+  if (w == 0) {
+    const unsigned v = seg_sum[l];
+    unsigned inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned t = __shfl_up_sync(0xffffffffu, inc, o);
+      if (l >= o) inc += t;
+    }
+    seg_sum[l] = inc - v;  // exclusive
+  }
+  __syncthreads();
+  unsigned run = seg_sum[w];
+  for (int c = beg; c < end; c += 32) {
+    const int i = c + l;
+    const unsigned v = i < end ? hist[i] : 0u;
+    unsigned inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned t = __shfl_up_sync(0xffffffffu, inc, o);
+      if (l >= o) inc += t;
+    }
+    if (i < end) hist[i] = run + inc - v;
+    run += __shfl_sync(0xffffffffu, inc, 31);
   }
 }
 
