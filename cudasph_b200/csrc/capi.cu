@@ -34,6 +34,7 @@ int launch_gravity(int n, const double4 *src, const double *h2src, double4 *out,
                    int precision, const int *mass_mixed, int rank, int world, cudaStream_t st);
 int launch_tree_gravity(const TreeView &t, const double4 *src, double4 *cm, double4 *q0, double4 *q1, double4 *out,
                         unsigned *flags, double eps, double theta, double G, int rank, int world, cudaStream_t st);
+long long gtree_nodes(int n);
 int launch_shard_pack(int n, int s0, int s1, const double4 *pos, const double4 *hyd, const double4 *dd,
                       const int *n_ngb, double4 *xbuf, cudaStream_t st);
 int launch_shard_unpack(int n, const double4 *xbuf, double4 *pos, double4 *hyd, double4 *dd, int *n_ngb,
@@ -343,9 +344,9 @@ extern "C" int cudasph_create(const sph_params *params, int n, int device, sph_c
   TRY_ALLOC(dalloc(&c->nevals, n));
   TRY_ALLOC(dalloc(&c->tlo, nodes));
   TRY_ALLOC(dalloc(&c->thi, nodes));
-  TRY_ALLOC(dalloc(&c->tcm, nodes));
-  TRY_ALLOC(dalloc(&c->tq0, nodes));
-  TRY_ALLOC(dalloc(&c->tq1, nodes));
+  TRY_ALLOC(dalloc(&c->tcm, (size_t)gtree_nodes(n)));
+  TRY_ALLOC(dalloc(&c->tq0, (size_t)gtree_nodes(n)));
+  TRY_ALLOC(dalloc(&c->tq1, (size_t)gtree_nodes(n)));
   TRY_ALLOC(dalloc(&c->keys, n));
   TRY_ALLOC(dalloc(&c->vals, n));
   TRY_ALLOC(dalloc((char **)&c->sort_scratch, radix_scratch_bytes(n)));
