@@ -653,16 +653,15 @@ def run_ours(args, rank, world):
         sim = Simulation(ic, make_params(**kw), device=dev)
         sim.step(2)
         sim.synchronize()
-        host_in = {k: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy() for k in ins}
-        host_out = {k: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy() for k in outs}
+        # two pinned host buffer sets; each step reads one and writes the other
+        bufs = [{k: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy() for k in outs} for _ in range(2)]
         for k in ins:
-            host_in[k][:] = sim.get(k)
-        sim.step_host(host_in, host_out)  # warm
+            bufs[0][k][:] = sim.get(k)
+        sim.step_host({k: bufs[0][k] for k in ins}, bufs[1])  # warm
         t0 = time.perf_counter()
-        for _ in range(args.e2e_steps):
-            for k in ins:
-                host_in[k][:] = host_out[k]
-            sim.step_host(host_in, host_out)
+        for i in range(args.e2e_steps):
+            src, dst = bufs[(i + 1) % 2], bufs[i % 2]
+            sim.step_host({k: src[k] for k in ins}, dst)
         e2e_s = time.perf_counter() - t0
         sim.close()
         out["e2e"] = {"value": n * args.e2e_steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 8 * n * len(ins),
@@ -739,23 +738,23 @@ def run_sharded(args, rank, world):
     if args.e2e_steps > 0:
         ins = ("x", "y", "z", "range", "vx", "vy", "vz", "m", "u", "mu", "ax", "ay", "az", "du")
         outs = ins + ("rho", "P")
-        host = {k: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy() for k in ins}
+        # two pinned host buffer sets; each step reads one and writes the other
+        bufs = [{k: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy() for k in outs} for _ in range(2)]
         for k in ins:
-            host[k][:] = sim.get(k)
+            bufs[0][k][:] = sim.get(k)
         dist.barrier()
         t0 = time.perf_counter()
-        for _ in range(args.e2e_steps):
-            sim.set_state(host)
+        for i in range(args.e2e_steps):
+            src, dst = bufs[i % 2], bufs[(i + 1) % 2]
+            sim.set_state_host({k: src[k] for k in ins})
             sim.step()
-            got = sim.get_state(outs)
-            for k in ins:
-                host[k][:] = got[k]
+            sim.get_state_host(dst)
         wall = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device="cuda")
         dist.all_reduce(wall, op=dist.ReduceOp.MAX)
         e2e = {"value": n * args.e2e_steps / float(wall.item()), "unit": UNIT, "h2d_bytes_per_step": 8 * n * len(ins),
                "d2h_bytes_per_step": 8 * n * len(outs), "steps": args.e2e_steps,
-               "api": "ShardedSimulation set_state / step / get_state (C ABI), pinned host buffers, wall clock, "
-                      "max over ranks, per rank"}
+               "api": "ShardedSimulation set_state_host / step / get_state_host (C ABI), pinned host buffers, "
+                      "wall clock, max over ranks, per rank"}
     sim.close()
     if rank != 0:
         return None
@@ -814,7 +813,19 @@ def run_reference(args, rank, world):
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def _json_stdout():
+    """The JSON line goes to the process's original stdout; everything else
+    written to file descriptor 1 from here on (libraries such as NCCL print
+    their version there at communicator init, the reference's CPU code prints
+    tree statistics) is sent to stderr, so stdout carries one JSON line."""
+    out = os.fdopen(os.dup(1), "w")
+    sys.stdout.flush()
+    os.dup2(2, 1)
+    return out
+
+
 def main():
+    json_out = _json_stdout()
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
@@ -841,13 +852,14 @@ def main():
                          "adjoint)")
     args = ap.parse_args()
     if args.large:
-        print(json.dumps({"measurement": "large_cold_sphere", **large_run()}), flush=True)
+        print(json.dumps({"measurement": "large_cold_sphere", **large_run()}), file=json_out, flush=True)
         return
     if args.c2:
-        print(json.dumps({"measurement": "fp64_262k_per_kernel", **c2_run()}), flush=True)
+        print(json.dumps({"measurement": "fp64_262k_per_kernel", **c2_run()}), file=json_out, flush=True)
         return
     if args.drift_steps > 0:
-        print(json.dumps({"measurement": "energy_drift", **energy_drift(args.n, args.drift_steps)}), flush=True)
+        print(json.dumps({"measurement": "energy_drift", **energy_drift(args.n, args.drift_steps)}), file=json_out,
+              flush=True)
         return
     assert args.warmup >= 3 or args.impl == "reference" or os.environ.get("BENCH_ALLOW_SHORT_WARMUP")
 
@@ -876,7 +888,7 @@ def main():
             import torch.distributed as dist
             dist.destroy_process_group()
     if out is not None and rank == 0:
-        print(json.dumps(out), flush=True)
+        print(json.dumps(out), file=json_out, flush=True)
 
 
 if __name__ == "__main__":

@@ -425,9 +425,10 @@ static void mark_changed(sph_ctx *c, int field) {
   }
 }
 
-extern "C" int cudasph_set_field(sph_ctx *c, int field, const double *src, int on_device) {
-  if (!c || !src || field < 0 || field >= SPH_NFIELDS) return SPH_ERR_ARG;
-  SPH_CUDA_TRY(cudaSetDevice(c->device));
+// One field in or out through the staging buffer `flat`, stream ordered: a
+// later copy into `flat` waits for the kernel that read it, so a run of
+// fields needs one host synchronisation at the end (for host memory).
+static int put_field(sph_ctx *c, int field, const double *src, int on_device) {
   int rc = copy_in(c, src, sizeof(double) * c->n, on_device, c->flat);
   if (rc) return rc;
   FieldRef r = field_ref(c, field);
@@ -435,6 +436,23 @@ extern "C" int cudasph_set_field(sph_ctx *c, int field, const double *src, int o
   c->launches++;
   mark_changed(c, field);
   SPH_CUDA_TRY(cudaGetLastError());
+  return SPH_OK;
+}
+
+static int take_field(sph_ctx *c, int field, double *dst, int on_device) {
+  FieldRef r = field_ref(c, field);
+  launch_field_io(c->n, r.base, r.stride, r.comp, c->f[c->cur].id, c->flat, 0, c->st);
+  c->launches++;
+  SPH_CUDA_TRY(cudaMemcpyAsync(dst, c->flat, sizeof(double) * c->n,
+                               on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, c->st));
+  return SPH_OK;
+}
+
+extern "C" int cudasph_set_field(sph_ctx *c, int field, const double *src, int on_device) {
+  if (!c || !src || field < 0 || field >= SPH_NFIELDS) return SPH_ERR_ARG;
+  SPH_CUDA_TRY(cudaSetDevice(c->device));
+  int rc = put_field(c, field, src, on_device);
+  if (rc) return rc;
   if (!on_device) SPH_CUDA_TRY(cudaStreamSynchronize(c->st));
   return SPH_OK;
 }
@@ -442,32 +460,33 @@ extern "C" int cudasph_set_field(sph_ctx *c, int field, const double *src, int o
 extern "C" int cudasph_get_field(sph_ctx *c, int field, double *dst, int on_device) {
   if (!c || !dst || field < 0 || field >= SPH_NFIELDS) return SPH_ERR_ARG;
   SPH_CUDA_TRY(cudaSetDevice(c->device));
-  FieldRef r = field_ref(c, field);
-  launch_field_io(c->n, r.base, r.stride, r.comp, c->f[c->cur].id, c->flat, 0, c->st);
-  c->launches++;
-  SPH_CUDA_TRY(cudaMemcpyAsync(dst, c->flat, sizeof(double) * c->n,
-                               on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, c->st));
+  int rc = take_field(c, field, dst, on_device);
+  if (rc) return rc;
   if (!on_device) SPH_CUDA_TRY(cudaStreamSynchronize(c->st));
   return SPH_OK;
 }
 
 extern "C" int cudasph_set_state(sph_ctx *c, const double *const *fields, int on_device) {
   if (!c || !fields) return SPH_ERR_ARG;
+  SPH_CUDA_TRY(cudaSetDevice(c->device));
   for (int k = 0; k < SPH_NFIELDS; k++) {
     if (!fields[k]) continue;
-    int rc = cudasph_set_field(c, k, fields[k], on_device);
+    int rc = put_field(c, k, fields[k], on_device);
     if (rc) return rc;
   }
+  if (!on_device) SPH_CUDA_TRY(cudaStreamSynchronize(c->st));
   return SPH_OK;
 }
 
 extern "C" int cudasph_get_state(sph_ctx *c, double *const *fields, int on_device) {
   if (!c || !fields) return SPH_ERR_ARG;
+  SPH_CUDA_TRY(cudaSetDevice(c->device));
   for (int k = 0; k < SPH_NFIELDS; k++) {
     if (!fields[k]) continue;
-    int rc = cudasph_get_field(c, k, fields[k], on_device);
+    int rc = take_field(c, k, fields[k], on_device);
     if (rc) return rc;
   }
+  if (!on_device) SPH_CUDA_TRY(cudaStreamSynchronize(c->st));
   return SPH_OK;
 }
 

@@ -171,17 +171,30 @@ class Simulation:
         else:
             check(lib().cudasph_steps(self._h, k), "steps")
 
+    @staticmethod
+    def _field_ptrs(fields: dict):
+        """pointer array of cudasph_set_state / get_state (float64 C-contiguous arrays)"""
+        p = (C.c_void_p * len(FIELDS))()
+        for k, i in FIELD_ID.items():
+            if k in fields:
+                a = fields[k]
+                if a.dtype != np.float64 or not a.flags.c_contiguous:
+                    raise ValueError(f"field {k}: a C-contiguous float64 array is required")
+                p[i] = a.ctypes.data
+        return p
+
     def step_host(self, fields_in: dict, fields_out: dict):
         """One step through host buffers (set_state + step + get_state)."""
-        nf = len(FIELDS)
-        pin = (C.c_void_p * nf)()
-        pout = (C.c_void_p * nf)()
-        for k, i in FIELD_ID.items():
-            if k in fields_in:
-                pin[i] = fields_in[k].ctypes.data
-            if k in fields_out:
-                pout[i] = fields_out[k].ctypes.data
-        check(lib().cudasph_step_host(self._h, pin, pout), "step_host")
+        check(lib().cudasph_step_host(self._h, self._field_ptrs(fields_in), self._field_ptrs(fields_out)),
+              "step_host")
+
+    def set_state_host(self, fields: dict):
+        """All given fields from host (or pinned) buffers in one call (one synchronisation)."""
+        check(lib().cudasph_set_state(self._h, self._field_ptrs(fields), 0), "set_state")
+
+    def get_state_host(self, fields: dict):
+        """All given fields into caller-owned host buffers in one call (one synchronisation)."""
+        check(lib().cudasph_get_state(self._h, self._field_ptrs(fields), 0), "get_state")
 
     def synchronize(self):
         self._call("synchronize")

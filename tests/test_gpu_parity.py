@@ -213,3 +213,28 @@ def test_graph_replay_matches_eager_steps():
         assert _rel(b.get(k), a.get(k)) < 1e-11, k
     assert abs(b.time - a.time) <= 1e-14 * abs(a.time)
     assert b.kernel_launches() == a.kernel_launches()
+
+
+def test_step_through_host_buffers_matches_the_resident_step(poly):
+    """cudasph_step_host (state in from host buffers, one step, state out, the
+    end-to-end path of the bench) and the batched set/get_state entries give
+    the same step as the device-resident handle."""
+    from cudasph_b200._capi import FIELDS
+    kw = dict(n_target=50.0, eos_mode=1, soft_mode=1, eps=0.01)
+    a = _sim(poly, **kw)
+    a.step()
+    ins = ("x", "y", "z", "range", "vx", "vy", "vz", "m", "u", "mu")
+    b = _sim(poly, **kw)
+    src = {k: np.ascontiguousarray(poly[k], np.float64) for k in ins}
+    out = {k: np.full(poly["x"].size, np.nan) for k in FIELDS}
+    b.step_host(src, out)
+    for k in ("x", "vx", "u", "range", "rho", "P", "ax", "du", "gx", "phi", "vsig"):
+        assert _rel(out[k], a.get(k)) < 1e-12, k
+    got = {k: np.empty(poly["x"].size) for k in ("x", "rho", "ax")}
+    b.get_state_host(got)
+    for k in got:
+        assert np.array_equal(got[k], out[k]), k
+    b.set_state_host({"u": 2 * out["u"]})
+    assert np.array_equal(b.get("u"), 2 * out["u"])
+    a.close()
+    b.close()
