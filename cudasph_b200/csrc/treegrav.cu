@@ -19,8 +19,8 @@
 // children, one per lane: a child is accepted for the whole group when
 // b < theta * dmin, dmin = distance from c to the group's box (so every
 // particle of the node lies at least (1 - theta) dmin from every target).
-// Accepted nodes go to a shared-memory list that all lanes sweep with the
-// softened monopole + quadrupole
+// Accepted nodes go to a shared-memory list that all lanes sweep, two nodes
+// per packed f32x2 instruction, with the softened monopole + quadrupole
 //   a = M r / s^3 - Q r / s^5 + (5/2) (r.Q.r) r / s^7,
 //   phi = -M / s - (1/2) (r.Q.r) / s^5,   r = c - x_i, s^2 = |r|^2 + eps^2;
 // opened level-0 nodes go to a list of source runs swept 32 particles at a
@@ -163,14 +163,17 @@ struct TreeGravArgs {
   int leaf0, leaf1;    // groups (SPH leaves) of this launch
 };
 
-struct NodeEntry {  // an accepted node, coordinates relative to the group anchor (3 x 16 B loads)
-  float4 pm;  // x, y, z, M
-  float4 qa;  // Qxx, Qyy, Qzz, Qxy
-  float4 qb;  // Qxz, Qyz, -, -
+// Accepted nodes are stored in pairs, component-interleaved so that one
+// packed f32x2 instruction advances both nodes of a pair against the lane's
+// target: pair j holds entries 2j and 2j+1 as {a0, a1} for each component
+// (coordinates relative to the group anchor), five 16-byte loads per pair.
+struct __align__(16) NodePair {
+  float x[2], y[2], z[2], m[2], qxx[2], qyy[2], qzz[2], qxy[2], qxz[2], qyz[2];
 };
+static_assert(sizeof(NodePair) == 80, "five 16-byte loads per pair");
 
 struct TgSmem {
-  NodeEntry list[kTgList];
+  NodePair list[kTgList / 2];
   float4 part[32];        // a sweep's staged source particles {x, y, z, m}
   int runs[kTgRuns];      // opened level-0 nodes awaiting their sweep
   int stack[kTgStack];
@@ -198,26 +201,53 @@ __global__ void __launch_bounds__(kTgWarps * 32) k_tree_gravity(TreeGravArgs a) 
   int nlist = 0, nruns = 0;
   bool ok = true;
 
+  const f32x2 X2 = pk2(xi, xi), Y2 = pk2(yi, yi), Z2 = pk2(zi, zi), E2 = pk2(eps2, eps2);
+  const f32x2 HALF5 = pk2(2.5f, 2.5f), MHALF = pk2(-0.5f, -0.5f), MONE = pk2(-1.f, -1.f);
   auto sweep_list = [&]() {
     __syncwarp();  // entries written by every lane are visible
-    float px = 0.f, py = 0.f, pz = 0.f, pp = 0.f;
-    for (int k = 0; k < nlist; k++) {
-      const float4 pm = sm.list[k].pm, qa = sm.list[k].qa, qb = sm.list[k].qb;
-      const float rx = pm.x - xi, ry = pm.y - yi, rz = pm.z - zi;
-      const float s2 = fmaf(rz, rz, fmaf(ry, ry, fmaf(rx, rx, eps2)));
-      const float inv = rsqrt_f32(s2), inv2 = inv * inv;
-      const float inv3 = inv2 * inv, inv5 = inv3 * inv2;
-      const float qx = qa.x * rx + qa.w * ry + qb.x * rz;
-      const float qy = qa.w * rx + qa.y * ry + qb.y * rz;
-      const float qz = qb.x * rx + qb.y * ry + qa.z * rz;
-      const float rqr = rx * qx + ry * qy + rz * qz;
-      const float c = pm.w * inv3 + 2.5f * rqr * inv5 * inv2;
-      px += c * rx - inv5 * qx;
-      py += c * ry - inv5 * qy;
-      pz += c * rz - inv5 * qz;
-      pp -= pm.w * inv + 0.5f * rqr * inv5;
+    if (nlist & 1) {  // pad an odd list with a massless node far away
+      if (lane == 0) {
+        NodePair &e = sm.list[nlist >> 1];
+        e.x[1] = e.y[1] = e.z[1] = 1e18f;
+        e.m[1] = e.qxx[1] = e.qyy[1] = e.qzz[1] = e.qxy[1] = e.qxz[1] = e.qyz[1] = 0.f;
+      }
+      __syncwarp();
     }
-    ax += px; ay += py; az += pz; ap += pp;
+    f32x2 px = 0ull, py = 0ull, pz = 0ull, pp = 0ull;
+    const int npair = (nlist + 1) >> 1;
+    for (int k = 0; k < npair; k++) {
+      const NodePair &e = sm.list[k];
+      const f32x2 ex = *reinterpret_cast<const f32x2 *>(e.x), ey = *reinterpret_cast<const f32x2 *>(e.y);
+      const f32x2 ez = *reinterpret_cast<const f32x2 *>(e.z), em = *reinterpret_cast<const f32x2 *>(e.m);
+      const f32x2 qxx = *reinterpret_cast<const f32x2 *>(e.qxx), qyy = *reinterpret_cast<const f32x2 *>(e.qyy);
+      const f32x2 qzz = *reinterpret_cast<const f32x2 *>(e.qzz), qxy = *reinterpret_cast<const f32x2 *>(e.qxy);
+      const f32x2 qxz = *reinterpret_cast<const f32x2 *>(e.qxz), qyz = *reinterpret_cast<const f32x2 *>(e.qyz);
+      const f32x2 rx = sub2(ex, X2), ry = sub2(ey, Y2), rz = sub2(ez, Z2);
+      f32x2 s2 = fma2(rx, rx, E2);
+      s2 = fma2(ry, ry, s2);
+      s2 = fma2(rz, rz, s2);
+      float sa, sb;
+      upk2(s2, sa, sb);
+      const f32x2 inv = pk2(rsqrt_f32(sa), rsqrt_f32(sb));
+      const f32x2 inv2 = mul2(inv, inv);
+      const f32x2 inv3 = mul2(inv2, inv), inv5 = mul2(inv3, inv2);
+      const f32x2 qx = fma2(qxz, rz, fma2(qxy, ry, mul2(qxx, rx)));
+      const f32x2 qy = fma2(qyz, rz, fma2(qyy, ry, mul2(qxy, rx)));
+      const f32x2 qz = fma2(qzz, rz, fma2(qyz, ry, mul2(qxz, rx)));
+      const f32x2 rqr = fma2(rz, qz, fma2(ry, qy, mul2(rx, qx)));
+      const f32x2 t = mul2(rqr, inv5);                          // (r.Q.r) / s^5
+      const f32x2 c = fma2(HALF5, mul2(t, inv2), mul2(em, inv3));  // M / s^3 + (5/2) (r.Q.r) / s^7
+      const f32x2 ni5 = mul2(inv5, MONE);
+      px = fma2(ni5, qx, fma2(c, rx, px));
+      py = fma2(ni5, qy, fma2(c, ry, py));
+      pz = fma2(ni5, qz, fma2(c, rz, pz));
+      pp = fma2(MHALF, t, sub2(pp, mul2(em, inv)));
+    }
+    float a0, a1;
+    upk2(px, a0, a1); ax += (double)a0 + (double)a1;
+    upk2(py, a0, a1); ay += (double)a0 + (double)a1;
+    upk2(pz, a0, a1); az += (double)a0 + (double)a1;
+    upk2(pp, a0, a1); ap += (double)a0 + (double)a1;
     nlist = 0;
     __syncwarp();  // every lane is done reading before the list is refilled
   };
@@ -303,11 +333,13 @@ __global__ void __launch_bounds__(kTgWarps * 32) k_tree_gravity(TreeGravArgs a) 
       if (accept) {
         const long long k = a.g.base[level] + child;
         const double4 qa = a.q0[k], qb = a.q1[k];
-        NodeEntry en;
-        en.pm = make_float4((float)(c.x - anc.x), (float)(c.y - anc.y), (float)(c.z - anc.z), (float)c.w);
-        en.qa = make_float4((float)qa.x, (float)qa.y, (float)qa.z, (float)qa.w);
-        en.qb = make_float4((float)qb.x, (float)qb.y, 0.f, 0.f);
-        sm.list[nlist + __popc(am & ((1u << lane) - 1u))] = en;
+        const int slot = nlist + __popc(am & ((1u << lane) - 1u));
+        NodePair &e = sm.list[slot >> 1];
+        const int h = slot & 1;
+        e.x[h] = (float)(c.x - anc.x); e.y[h] = (float)(c.y - anc.y); e.z[h] = (float)(c.z - anc.z);
+        e.m[h] = (float)c.w;
+        e.qxx[h] = (float)qa.x; e.qyy[h] = (float)qa.y; e.qzz[h] = (float)qa.z; e.qxy[h] = (float)qa.w;
+        e.qxz[h] = (float)qb.x; e.qyz[h] = (float)qb.y;
       }
       nlist += __popc(am);
       __syncwarp();
