@@ -7,8 +7,9 @@ all-reduce does across GPUs.  Kernels of different shards never wait on one
 another: each exchange synchronizes every shard's stream first.  The result
 must equal the unsharded step (neighbour counts exactly; FP64 fields to the
 rounding of FP64 atomics added in another order), and all shards must hold
-bit-identical state.  A one-rank NCCL process group runs the same protocol
-through torch.distributed on the context's stream.
+bit-identical state; FP64, mixed, unequal masses, spline softening and the
+tree gravity are covered.  A one-rank NCCL process group runs the same
+protocol through torch.distributed on the context's stream.
 """
 import numpy as np
 import pytest
@@ -59,12 +60,13 @@ def _rel(a, b):
 
 
 @pytest.mark.parametrize("world", [2, 3])
-@pytest.mark.parametrize("precision,soft,equal", [(0, 1, True), (1, 1, True), (1, 1, False), (1, 0, True)])
-def test_lockstep_shards_equal_unsharded_step(world, precision, soft, equal):
+@pytest.mark.parametrize("precision,soft,equal,grav", [(0, 1, True, 0), (1, 1, True, 0), (1, 1, False, 0),
+                                                       (1, 0, True, 0), (1, 1, True, 1)])
+def test_lockstep_shards_equal_unsharded_step(world, precision, soft, equal, grav):
     from cudasph_b200.sharded import ShardedSimulation
     from cudasph_b200.simulation import Simulation, make_params
     ic = _ic(equal=equal)
-    par = dict(precision=precision, n_target=50.0, eos_mode=1, soft_mode=soft, eps=0.01)
+    par = dict(precision=precision, n_target=50.0, eos_mode=1, soft_mode=soft, eps=0.01, grav_mode=grav)
     ref = Simulation(ic, make_params(**par))
     shards = [ShardedSimulation(ic, make_params(**par), r, world) for r in range(world)]
     ref.step()
