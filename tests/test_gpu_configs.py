@@ -41,6 +41,28 @@ def test_c1_ten_fp64_steps_match_the_oracle():
     assert sim.device_status() & 0x7 == 0
 
 
+def test_c1_neighbour_number_within_two_of_the_target():
+    """N_ngb is the reference's smoothed neighbour number sum_j ig(2 r_ij /
+    range_i) (dev_solve_range.cu:68), which the h solve drives to the
+    target: after ten steps of C1 it must lie within 50 +- 2 for every
+    particle (the solve's 1e-3 tolerance in range keeps it within about
+    +- 0.15).  The hard count inside the range is larger, since ig weighs the
+    outer shell below 1."""
+    ic = ics.polytrope(16384, n_poly=1.5, n_ngb=50.0, seed=12345 + 1)
+    kw = dict(n_target=50.0, eos_mode=0, soft_mode=1, eps=0.01, av_alpha=1.0, av_beta=2.0)
+    sim = _sim(ic, **kw)
+    sim.step(10)
+    sim.CUDA_solve_range()
+    x, y, z, rng = (sim.get(k) for k in ("x", "y", "z", "range"))
+    cnt, off, lst = sim.neighbours()
+    i = np.repeat(np.arange(x.size), cnt)
+    r = np.sqrt((x[i] - x[lst]) ** 2 + (y[i] - y[lst]) ** 2 + (z[i] - z[lst]) ** 2)
+    smooth = np.bincount(i, weights=O.kernel_eval("ig", 2 * r / rng[i]), minlength=x.size)
+    assert np.all(np.abs(smooth - 50.0) <= 2.0), (smooth.min(), smooth.max())
+    assert np.max(np.abs(smooth - 50.0)) < 0.5
+    assert cnt.mean() > 50.0
+
+
 def test_c2_sort_and_neighbour_sets_bitexact():
     n = 262144
     ic = ics.polytrope(n, n_poly=1.5, n_ngb=64.0, seed=12345 + 2, u_jitter=0.05, mu=0.62)
