@@ -133,19 +133,38 @@ def gpu_uuid():
 
 # ----------------------------------------------------------------------------
 def time_steps(sim, steps, warmup):
-    """Device time of `steps` whole steps (CUDA events on the context stream)."""
+    """Device time of `steps` whole steps: CUDA events on the context's
+    stream around them (the whole span, gaps between launches included),
+    plus the per-phase device times for the breakdown."""
+    import torch
     sim.step(warmup)
     sim.synchronize()
     sim.reset_counters()
     sim.set_profiling(True)
+    st = sim.torch_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t0 = time.perf_counter()
+    e0.record(st)
     sim.step(steps)
-    sim.synchronize()
+    e1.record(st)
+    e1.synchronize()
     wall = time.perf_counter() - t0
     ph = sim.phase_times()
     sim.set_profiling(False)
-    dev_ms = sum(v[0] for v in ph.values())
+    dev_ms = e0.elapsed_time(e1)
     return dev_ms, wall, ph, sim.kernel_launches()
+
+
+def step_span_ms(sim, k=1):
+    """CUDA-event span of k whole steps on the context's stream."""
+    import torch
+    st = sim.torch_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    sim.step(k)
+    e1.record(st)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
 
 
 def rms_rel(a, b):
@@ -239,10 +258,11 @@ def adjoint_cost(steps=5, warmup=3, headline_n=None):
     ic = ics.polytrope(ADJOINT_N, n_poly=3.0, n_ngb=50.0, seed=12345 + 4, mu=0.62)
     out = {"workload": f"n=3 polytrope, N={ADJOINT_N}, gas+radiation EOS mu=0.62, N_ngb=50, Plummer eps=0.01"}
     def step_and_adjoint(sim, m):
-        sim.step()
+        fwd = step_span_ms(sim)
         for k in ("vx", "vy", "vz"):
             sim.adjoint_set(k, m * sim.get(k))
         sim.adjoint()
+        return fwd
 
     for name, prec in (("fp64", 0), ("mixed", 1)):
         sim = Simulation(ic, make_params(precision=prec, **ADJOINT_PARAMS))
@@ -255,10 +275,9 @@ def adjoint_cost(steps=5, warmup=3, headline_n=None):
             sim.synchronize()
             sim.reset_counters()
             sim.set_profiling(True)
-            step_and_adjoint(sim, m)
+            fwd_s.append(step_and_adjoint(sim, m))
             ph = sim.phase_times()
             sim.set_profiling(False)
-            fwd_s.append(sum(v[0] for k, v in ph.items() if k != "adjoint"))
             adj_s.append(ph["adjoint"][0])
         fwd, adj = float(np.median(fwd_s)), float(np.median(adj_s))
         out[name] = {"forward_ms": fwd, "adjoint_ms": adj, "adjoint_over_forward": adj / fwd,
@@ -276,14 +295,9 @@ def adjoint_cost(steps=5, warmup=3, headline_n=None):
         sim.synchronize()
         sim.reset_counters()
         sim.set_profiling(True)
-        sim.step()
-        m = ic["m"]
-        for k in ("vx", "vy", "vz"):
-            sim.adjoint_set(k, m * sim.get(k))
-        sim.adjoint()
+        fwd = step_and_adjoint(sim, ic["m"])
         ph = sim.phase_times()
         sim.set_profiling(False)
-        fwd = sum(v[0] for k, v in ph.items() if k != "adjoint")
         adj = ph["adjoint"][0]
         out["headline_workload_mixed"] = {"n": headline_n, "forward_ms": fwd, "adjoint_ms": adj,
                                           "adjoint_over_forward": adj / fwd,
@@ -378,12 +392,10 @@ def large_run(n=LARGE_N, steps=5, n_sub=262144):
     sim = Simulation(ic, make_params(precision=1, **LARGE_PARAMS))
     sim.reset_counters()
     sim.set_profiling(True)
-    sim.step(steps)
-    sim.synchronize()
+    step_ms = step_span_ms(sim, steps) / steps
     ph = sim.phase_times()
     sim.set_profiling(False)
     gms = ph["gravity"][0] / steps
-    step_ms = sum(v[0] for v in ph.values()) / steps
     res["ms_per_step"] = step_ms
     res["particle_steps_per_s"] = n / (step_ms * 1e-3)
     res["phase_ms_per_step"] = {k: round(v[0] / steps, 3) for k, v in ph.items()}
@@ -414,14 +426,13 @@ def large_run(n=LARGE_N, steps=5, n_sub=262144):
     s2.synchronize()
     s2.reset_counters()
     s2.set_profiling(True)
-    s2.step()
+    fwd = step_span_ms(s2)
     for k in ("vx", "vy", "vz"):
         s2.adjoint_set(k, m * s2.get(k))
     s2.adjoint()
     s2.synchronize()
     ph2 = s2.phase_times()
     s2.set_profiling(False)
-    fwd = sum(v[0] for k, v in ph2.items() if k != "adjoint")
     adj = ph2["adjoint"][0]
     res["adjoint_subset"] = {"n": n_sub, "forward_ms": fwd, "adjoint_ms": adj, "adjoint_over_forward": adj / fwd,
                              "loss": "kinetic energy after the step", "device_flags": s2.device_status()}

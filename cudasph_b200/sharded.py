@@ -82,15 +82,6 @@ class ShardedSimulation(Simulation):
         check(lib().cudasph_device_buffer(self._h, BUFFERS[name], C.byref(ptr), C.byref(cnt)), "device_buffer")
         return torch.as_tensor(_DeviceArray(ptr.value, cnt.value), device=f"cuda:{self.device}")
 
-    def torch_stream(self):
-        """the context's stream as a torch stream (collectives are ordered on it)"""
-        if self._stream is None:
-            import torch
-            s = C.c_void_p()
-            check(lib().cudasph_get_stream(self._h, C.byref(s)), "get_stream")
-            self._stream = torch.cuda.ExternalStream(s.value or 0, device=f"cuda:{self.device}")
-        return self._stream
-
     def stages(self):
         """One step as a generator: runs the phases up to each exchange and
         yields the names of the buffers to sum over the ranks there."""

@@ -199,6 +199,16 @@ class Simulation:
     def synchronize(self):
         self._call("synchronize")
 
+    def torch_stream(self):
+        """The context's CUDA stream as a torch stream (events and collectives
+        ordered with the context's work are recorded on it)."""
+        if getattr(self, "_stream", None) is None:
+            import torch
+            s = C.c_void_p()
+            check(lib().cudasph_get_stream(self._h, C.byref(s)), "get_stream")
+            self._stream = torch.cuda.ExternalStream(s.value or 0, device=f"cuda:{self.device}")
+        return self._stream
+
     def system_statistics(self) -> dict:
         out = np.empty(len(STATS), np.float64)
         check(lib().cudasph_statistics(self._h, out.ctypes.data), "statistics")
