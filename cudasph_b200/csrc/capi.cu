@@ -32,9 +32,9 @@ int launch_density_mixed(const HydroArgs &a, cudaStream_t st);
 int launch_hydro_mixed(const HydroArgs &a, cudaStream_t st);
 int launch_gravity(int n, const double4 *src, const double *h2src, double4 *out, int soft_mode, double eps, double G,
                    int precision, const int *mass_mixed, int rank, int world, cudaStream_t st);
-int launch_tree_gravity(const TreeView &t, const double4 *src, double4 *cm, double4 *q0, double4 *q1, double4 *out,
+int launch_tree_gravity(const TreeView &t, const uint64_t *keys, const double4 *src, void *ws, double4 *out,
                         unsigned *flags, double eps, double theta, double G, int rank, int world, cudaStream_t st);
-long long gtree_nodes(int n);
+size_t tree_gravity_workspace_bytes(int n);
 int launch_shard_pack(int n, int s0, int s1, const double4 *pos, const double4 *hyd, const double4 *dd,
                       const int *n_ngb, double4 *xbuf, cudaStream_t st);
 int launch_shard_unpack(int n, const double4 *xbuf, double4 *pos, double4 *hyd, double4 *dd, int *n_ngb,
@@ -87,7 +87,7 @@ struct sph_ctx {
   double *dcache = nullptr;  // candidate squared distances of the h solve, layout of list
   TreeView tree;
   float4 *tlo = nullptr, *thi = nullptr;
-  double4 *tcm = nullptr, *tq0 = nullptr, *tq1 = nullptr;  // tree-gravity node moments
+  void *tgws = nullptr;  // tree-gravity workspace (radix tree + node moments)
   uint64_t *keys = nullptr;
   uint32_t *vals = nullptr;
   void *sort_scratch = nullptr;
@@ -289,7 +289,7 @@ extern "C" int cudasph_destroy(sph_ctx *c) {
     cudaFree(F.vsig); cudaFree(F.id);
   }
   cudaFree(c->old); cudaFree(c->n_ngb); cudaFree(c->nevals); cudaFree(c->list); cudaFree(c->dcache);
-  cudaFree(c->tlo); cudaFree(c->thi); cudaFree(c->tcm); cudaFree(c->tq0); cudaFree(c->tq1); cudaFree(c->keys); cudaFree(c->vals); cudaFree(c->sort_scratch);
+  cudaFree(c->tlo); cudaFree(c->thi); cudaFree(c->tgws); cudaFree(c->keys); cudaFree(c->vals); cudaFree(c->sort_scratch);
   cudaFree(c->bbox_part); cudaFree(c->box4); cudaFree(c->gsrc); cudaFree(c->gh2); cudaFree(c->mass_mixed); cudaFree(c->xbuf); cudaFree(c->flags);
   cudaFree(c->sc); cudaFree(c->fin_part); cudaFree(c->flat); cudaFree(c->slot_of);
   cudaFree(c->pre_acc); cudaFree(c->xb); cudaFree(c->vb); cudaFree(c->ab); cudaFree(c->vpb); cudaFree(c->vpup);
@@ -344,9 +344,7 @@ extern "C" int cudasph_create(const sph_params *params, int n, int device, sph_c
   TRY_ALLOC(dalloc(&c->nevals, n));
   TRY_ALLOC(dalloc(&c->tlo, nodes));
   TRY_ALLOC(dalloc(&c->thi, nodes));
-  TRY_ALLOC(dalloc(&c->tcm, (size_t)gtree_nodes(n)));
-  TRY_ALLOC(dalloc(&c->tq0, (size_t)gtree_nodes(n)));
-  TRY_ALLOC(dalloc(&c->tq1, (size_t)gtree_nodes(n)));
+  TRY_ALLOC(dalloc((char **)&c->tgws, tree_gravity_workspace_bytes(n)));
   TRY_ALLOC(dalloc(&c->keys, n));
   TRY_ALLOC(dalloc(&c->vals, n));
   TRY_ALLOC(dalloc((char **)&c->sort_scratch, radix_scratch_bytes(n)));
@@ -708,8 +706,9 @@ extern "C" int cudasph_gravity(sph_ctx *c) {
   Fields &F = c->f[c->cur];
   if (c->p.grav_mode == SPH_GRAV_TREE) {
     LAUNCHED(launch_pack_sources(c->n, F.pos, F.vel, c->gsrc, c->gh2, c->mass_mixed, c->st));
-    LAUNCHED(launch_tree_gravity(c->tree, c->gsrc, c->tcm, c->tq0, c->tq1, F.grav, c->flags, c->p.eps, c->p.theta,
-                                 c->p.G, c->rank, c->world, c->st));
+    // the radix tree is built from the sort's keys, which match the current order
+    LAUNCHED(launch_tree_gravity(c->tree, c->keys, c->gsrc, c->tgws, F.grav, c->flags, c->p.eps, c->p.theta, c->p.G,
+                                 c->rank, c->world, c->st));
     SPH_CUDA_TRY(cudaGetLastError());
     return SPH_OK;
   }

@@ -5,157 +5,195 @@
 // this mode trades a bounded force error (set by the opening angle theta)
 // for O(N log N) work.
 //
-// Source tree: its own implicit hierarchy over the Morton order, finer than
-// the SPH tree: level 0 nodes are runs of 8 consecutive particles, every
-// level above groups 8 consecutive nodes.  Every node gets its mass M,
-// centre of mass c, traceless quadrupole Q_ab = sum m (3 d_a d_b - |d|^2
-// delta_ab) (d = x - c) and radius b = max |x - c|, all in FP64: level 0 from
-// its particles, parents from their 8 children by the parallel-axis shift
-// Q += M_k (3 s s - |s|^2 I), s = c_k - c, and b = max(|s| + b_k).  Eight
-// lanes build one node (four nodes per warp).
+// Source tree: the binary radix tree of the sorted Morton keys (each
+// internal node covers a contiguous run of particles that share a key
+// prefix and splits it where the next key bit changes, so every node is a
+// compact Morton cell or a half of one; equal keys split by index).  One
+// thread per internal node finds its range and split from the keys alone
+// (binary searches on common-prefix lengths).  Moments -- mass M, centre of
+// mass c, traceless quadrupole Q_ab = sum m (3 d_a d_b - |d|^2 delta_ab)
+// (d = x - c) and radius b = max |x - c| -- are FP64 and built bottom-up: one
+// thread per particle climbs towards the root, and at every node the second
+// of its two children's threads to arrive combines them (parallel-axis shift
+// Q += M_k (3 s s - |s|^2 I), s = c_k - c; b = max(|s| + b_k)).
 //
 // Walk: one warp per SPH leaf (a "group" of 32 targets, whose float box the
-// SPH tree holds).  Each round pops up to four nodes and tests their 8
-// children, one per lane: a child is accepted for the whole group when
-// b < theta * dmin, dmin = distance from c to the group's box (so every
-// particle of the node lies at least (1 - theta) dmin from every target).
-// Accepted nodes go to a shared-memory list that all lanes sweep, two nodes
-// per packed f32x2 instruction, with the softened monopole + quadrupole
+// SPH tree holds).  Each round pops up to sixteen internal nodes and tests
+// their two children, one per lane: a child node is accepted for the whole
+// group when b < theta * dmin, dmin = distance from c to the group's box (so
+// every particle of the node lies at least (1 - theta) dmin from every
+// target).  Accepted nodes go to a shared-memory list that all lanes sweep,
+// two nodes per packed f32x2 instruction, with the softened monopole +
+// quadrupole
 //   a = M r / s^3 - Q r / s^5 + (5/2) (r.Q.r) r / s^7,
 //   phi = -M / s - (1/2) (r.Q.r) / s^5,   r = c - x_i, s^2 = |r|^2 + eps^2;
-// opened level-0 nodes go to a list of source runs swept 32 particles at a
-// time with the Plummer pair term of the direct kernels; opened higher nodes
-// are pushed.  Pair terms are FP32 on coordinates relative to the group's
-// first particle (FP64 anchor); each sweep's FP32 partials fold into FP64.
+// child particles and opened nodes of at most kBucket particles go to a ring
+// of source particles swept 32 at a time with the Plummer pair term of the
+// direct kernels; larger opened nodes are pushed.  Pair terms are FP32 on
+// coordinates relative to the group's first particle (FP64 anchor); each
+// sweep's FP32 partials fold into FP64.
+#include <cstdint>
+
 #include "common.cuh"
 #include "pairmath.cuh"
 
 namespace sph {
 
-constexpr int kGFan = 8;        // children per gravity-tree node, particles per level-0 node
-constexpr int kGLevels = 12;    // supports up to 8^12 particles
 constexpr int kTgWarps = 4;     // warps (groups) per block
 constexpr int kTgList = 96;     // accepted-node list entries per warp
-constexpr int kTgRuns = 64;     // opened level-0 runs buffered per warp (a round opens at most 32)
-constexpr int kTgStack = 512;   // traversal stack entries per warp
+constexpr int kTgRing = 512;    // source-particle ring per warp (a round adds at most 32 * kBucket)
+constexpr int kTgStack = 1024;  // traversal stack entries per warp
+constexpr int kBucket = 8;      // an opened node of at most this many particles is summed particle by particle
+static_assert(32 * kBucket + 32 <= kTgRing, "a round's particles fit the ring");
 
-struct GTree {
-  int levels;
-  int count[kGLevels];
-  long long base[kGLevels];
+// ------------------------------- workspace ----------------------------------
+// per internal node (n - 1 of them): moments cm = {cx, cy, cz, M},
+// q0 = {Qxx, Qyy, Qzz, Qxy}, q1 = {Qxz, Qyz, b, count}; children (an index
+// >= 0 is an internal node, ~p a particle); particle range; parent; arrival
+// counter of the bottom-up pass.  Per particle: its parent.
+struct TgWork {
+  double4 *cm, *q0, *q1;
+  int2 *child, *range;
+  int *parent, *lparent;
+  unsigned *flag;
 };
 
-static GTree gtree_layout(int n) {
-  GTree g;
-  long long off = 0;
-  int c = (n + kGFan - 1) / kGFan;
-  if (c < 1) c = 1;
-  g.levels = 0;
-  while (true) {
-    g.count[g.levels] = c;
-    g.base[g.levels] = off;
-    off += c;
-    g.levels++;
-    if (c == 1 || g.levels == kGLevels) break;
-    c = (c + kGFan - 1) / kGFan;
+static size_t al256(size_t b) { return (b + 255) / 256 * 256; }
+
+size_t tree_gravity_workspace_bytes(int n) {
+  const size_t ni = n > 1 ? (size_t)n - 1 : 1;
+  return 3 * al256(sizeof(double4) * ni) + 2 * al256(sizeof(int2) * ni) + al256(sizeof(int) * ni) +
+         al256(sizeof(int) * (size_t)(n > 0 ? n : 1)) + al256(sizeof(unsigned) * ni);
+}
+
+static TgWork carve(void *ws, int n) {
+  const size_t ni = n > 1 ? (size_t)n - 1 : 1;
+  char *p = (char *)ws;
+  TgWork w;
+  w.cm = (double4 *)p; p += al256(sizeof(double4) * ni);
+  w.q0 = (double4 *)p; p += al256(sizeof(double4) * ni);
+  w.q1 = (double4 *)p; p += al256(sizeof(double4) * ni);
+  w.child = (int2 *)p; p += al256(sizeof(int2) * ni);
+  w.range = (int2 *)p; p += al256(sizeof(int2) * ni);
+  w.parent = (int *)p; p += al256(sizeof(int) * ni);
+  w.lparent = (int *)p; p += al256(sizeof(int) * (size_t)(n > 0 ? n : 1));
+  w.flag = (unsigned *)p;
+  return w;
+}
+
+// ------------------------------- topology ------------------------------------
+// common-prefix length of keys i and j (64 + that of the indices for equal
+// keys, -1 outside [0, n))
+__device__ __forceinline__ int prefix(const uint64_t *__restrict__ k, int n, int i, int j) {
+  if (j < 0 || j >= n) return -1;
+  const uint64_t a = k[i], b = k[j];
+  if (a == b) return 64 + __clz((unsigned)(i ^ j));
+  return __clzll((long long)(a ^ b));
+}
+
+__global__ void k_radix_tree(int n, const uint64_t *__restrict__ keys, TgWork w) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n - 1) return;
+  // direction of the node's range and its length by exponential + binary search
+  const int d = prefix(keys, n, i, i + 1) - prefix(keys, n, i, i - 1) >= 0 ? 1 : -1;
+  const int dmin = prefix(keys, n, i, i - d);
+  int lmax = 2;
+  while (prefix(keys, n, i, i + lmax * d) > dmin) lmax <<= 1;
+  int l = 0;
+  for (int t = lmax >> 1; t >= 1; t >>= 1)
+    if (prefix(keys, n, i, i + (l + t) * d) > dmin) l += t;
+  const int j = i + l * d;
+  // the split: the last position sharing more than the node's common prefix
+  const int dnode = prefix(keys, n, i, j);
+  int s = 0;
+  for (int div = 2;; div <<= 1) {
+    const int t = (l + div - 1) / div;
+    if (prefix(keys, n, i, i + (s + t) * d) > dnode) s += t;
+    if (t == 1) break;
   }
-  return g;
+  const int gamma = i + s * d + min(d, 0);
+  const int lo = min(i, j), hi = max(i, j);
+  const int left = (lo == gamma) ? ~gamma : gamma;
+  const int right = (hi == gamma + 1) ? ~(gamma + 1) : gamma + 1;
+  w.child[i] = make_int2(left, right);
+  w.range[i] = make_int2(lo, hi);
+  if (left < 0) w.lparent[gamma] = i;
+  else w.parent[gamma] = i;
+  if (right < 0) w.lparent[gamma + 1] = i;
+  else w.parent[gamma + 1] = i;
+  if (i == 0) w.parent[0] = -1;  // node 0 covers [0, n) and is the root
+  w.flag[i] = 0u;
 }
 
-// nodes of the gravity tree over n particles (moment arrays hold this many)
-long long gtree_nodes(int n) {
-  const GTree g = gtree_layout(n);
-  return g.base[g.levels - 1] + g.count[g.levels - 1];
+// a child's moments: a particle {x, m}, or an internal node written by
+// another thread of this launch (read from L2, past the incoherent L1)
+__device__ __forceinline__ void child_moments(int ref, const double4 *__restrict__ src, const TgWork &w, double4 &c,
+                                              double4 &qa, double4 &qb) {
+  if (ref < 0) {
+    c = src[~ref];
+    qa = make_double4(0, 0, 0, 0);
+    qb = make_double4(0, 0, 0, 1);
+    return;
+  }
+  const double2 *pc = reinterpret_cast<const double2 *>(w.cm + ref);
+  const double2 *pa = reinterpret_cast<const double2 *>(w.q0 + ref);
+  const double2 *pb = reinterpret_cast<const double2 *>(w.q1 + ref);
+  const double2 c0 = __ldcg(pc), c1 = __ldcg(pc + 1), a0 = __ldcg(pa), a1 = __ldcg(pa + 1), b0 = __ldcg(pb),
+                b1 = __ldcg(pb + 1);
+  c = make_double4(c0.x, c0.y, c1.x, c1.y);
+  qa = make_double4(a0.x, a0.y, a1.x, a1.y);
+  qb = make_double4(b0.x, b0.y, b1.x, b1.y);
 }
 
-// ------------------------------- moments ------------------------------------
-// sums over the 8 lanes of a node (lanes 8k .. 8k+7)
-__device__ __forceinline__ double seg_sum(double v) {
-#pragma unroll
-  for (int o = 4; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-__device__ __forceinline__ double seg_max(double v) {
-#pragma unroll
-  for (int o = 4; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-  return v;
-}
-
-// cm = {cx, cy, cz, M}; q0 = {Qxx, Qyy, Qzz, Qxy}; q1 = {Qxz, Qyz, b, 0}.
-// Level 0 (parent = false): member k of node `node` is particle 8 node + k
-// with src = {x, y, z, m}.  Parents: member k is child node 8 node + k of
-// the level below, read from (ccm, cq0, cq1).
-template <bool PARENT>
-__global__ void k_gtree_moments(int nmember, int nnode, const double4 *__restrict__ src,
-                                const double4 *__restrict__ ccm, const double4 *__restrict__ cq0,
-                                const double4 *__restrict__ cq1, double4 *__restrict__ cm, double4 *__restrict__ q0,
-                                double4 *__restrict__ q1) {
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-  const int node = tid >> 3, k = tid & 7;
-  // every lane of the warp takes part in the shuffles; nodes past the end are empty
-  const bool live = node < nnode;
-  const int mbr = node * kGFan + k;
-  double4 m = make_double4(0, 0, 0, 0), a = m, b4 = m;
-  if (live && mbr < nmember) {
-    if (PARENT) {
-      m = ccm[mbr];
-      a = cq0[mbr];
-      b4 = cq1[mbr];
+__global__ void k_tree_moments(int n, const double4 *__restrict__ src, TgWork w) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  int node = w.lparent[p];
+  while (node >= 0) {
+    __threadfence();  // this thread's node writes (previous pass) before its arrival count
+    if (atomicAdd(&w.flag[node], 1u) == 0u) return;  // the other child's thread combines
+    const int2 ch = w.child[node];
+    double4 ca, qaa, qab, cb, qba, qbb;
+    child_moments(ch.x, src, w, ca, qaa, qab);
+    child_moments(ch.y, src, w, cb, qba, qbb);
+    const double M = ca.w + cb.w;
+    double cx, cy, cz;
+    if (M > 0) {
+      cx = (ca.w * ca.x + cb.w * cb.x) / M;
+      cy = (ca.w * ca.y + cb.w * cb.y) / M;
+      cz = (ca.w * ca.z + cb.w * cb.z) / M;
     } else {
-      m = src[mbr];
+      cx = ca.x; cy = ca.y; cz = ca.z;
     }
+    double Q[6] = {qaa.x + qba.x, qaa.y + qba.y, qaa.z + qba.z, qaa.w + qba.w, qab.x + qbb.x, qab.y + qbb.y};
+    double b = 0;
+    const double4 *cs[2] = {&ca, &cb};
+    const double bs[2] = {qab.z, qbb.z};
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+      const double4 &ck = *cs[k];
+      const double sx = ck.x - cx, sy = ck.y - cy, sz = ck.z - cz, s2 = sx * sx + sy * sy + sz * sz;
+      Q[0] += ck.w * (3 * sx * sx - s2);
+      Q[1] += ck.w * (3 * sy * sy - s2);
+      Q[2] += ck.w * (3 * sz * sz - s2);
+      Q[3] += ck.w * 3 * sx * sy;
+      Q[4] += ck.w * 3 * sx * sz;
+      Q[5] += ck.w * 3 * sy * sz;
+      if (ck.w > 0) b = fmax(b, sqrt(s2) + bs[k]);
+    }
+    const int2 r = w.range[node];
+    w.cm[node] = make_double4(cx, cy, cz, M);
+    w.q0[node] = make_double4(Q[0], Q[1], Q[2], Q[3]);
+    w.q1[node] = make_double4(Q[4], Q[5], b, (double)(r.y - r.x + 1));
+    node = w.parent[node];
   }
-  const double M = seg_sum(m.w);
-  double cx = seg_sum(m.w * m.x), cy = seg_sum(m.w * m.y), cz = seg_sum(m.w * m.z);
-  const int first = (int)(lane_id() & ~7u);
-  if (M > 0) {
-    cx /= M; cy /= M; cz /= M;
-  } else {  // massless node: centre at its first member
-    cx = __shfl_sync(0xffffffffu, m.x, first);
-    cy = __shfl_sync(0xffffffffu, m.y, first);
-    cz = __shfl_sync(0xffffffffu, m.z, first);
-  }
-  const double sx = m.x - cx, sy = m.y - cy, sz = m.z - cz, s2 = sx * sx + sy * sy + sz * sz;
-  double Q[6];
-  Q[0] = seg_sum(a.x + m.w * (3 * sx * sx - s2));
-  Q[1] = seg_sum(a.y + m.w * (3 * sy * sy - s2));
-  Q[2] = seg_sum(a.z + m.w * (3 * sz * sz - s2));
-  Q[3] = seg_sum(a.w + m.w * 3 * sx * sy);
-  Q[4] = seg_sum(b4.x + m.w * 3 * sx * sz);
-  Q[5] = seg_sum(b4.y + m.w * 3 * sy * sz);
-  const double b = seg_max((live && mbr < nmember && m.w > 0) ? sqrt(s2) + (PARENT ? b4.z : 0.0) : 0.0);
-  if (live && k == 0) {
-    cm[node] = make_double4(cx, cy, cz, M);
-    q0[node] = make_double4(Q[0], Q[1], Q[2], Q[3]);
-    q1[node] = make_double4(Q[4], Q[5], b, 0.0);
-  }
-}
-
-static int gtree_moments(const GTree &g, int n, const double4 *src, double4 *cm, double4 *q0, double4 *q1,
-                         cudaStream_t st) {
-  int launches = 0;
-  {
-    const int nn = g.count[0];
-    k_gtree_moments<false><<<(nn * kGFan + 255) / 256, 256, 0, st>>>(n, nn, src, nullptr, nullptr, nullptr,
-                                                                     cm + g.base[0], q0 + g.base[0], q1 + g.base[0]);
-    launches++;
-  }
-  for (int l = 1; l < g.levels; l++) {
-    const int nn = g.count[l];
-    k_gtree_moments<true><<<(nn * kGFan + 255) / 256, 256, 0, st>>>(
-        g.count[l - 1], nn, nullptr, cm + g.base[l - 1], q0 + g.base[l - 1], q1 + g.base[l - 1], cm + g.base[l],
-        q0 + g.base[l], q1 + g.base[l]);
-    launches++;
-  }
-  return launches;
 }
 
 // -------------------------------- the walk -----------------------------------
 struct TreeGravArgs {
   TreeView t;          // the SPH tree: the groups' boxes (level 0)
-  GTree g;             // the gravity tree
+  TgWork w;            // the gravity tree
   const double4 *src;  // {x, y, z, m} per particle, tree order
-  const double4 *cm, *q0, *q1;
   double4 *out;        // {gx, gy, gz, phi}
   unsigned *flags;
   float eps2, theta;
@@ -174,9 +212,9 @@ static_assert(sizeof(NodePair) == 80, "five 16-byte loads per pair");
 
 struct TgSmem {
   NodePair list[kTgList / 2];
-  float4 part[32];        // a sweep's staged source particles {x, y, z, m}
-  int runs[kTgRuns];      // opened level-0 nodes awaiting their sweep
-  int stack[kTgStack];
+  float4 part[32];       // a sweep's staged source particles {x, y, z, m}
+  int ring[kTgRing];     // source particles awaiting their sweep
+  int stack[kTgStack];   // internal nodes to open
 };
 
 __global__ void __launch_bounds__(kTgWarps * 32) k_tree_gravity(TreeGravArgs a) {
@@ -198,7 +236,8 @@ __global__ void __launch_bounds__(kTgWarps * 32) k_tree_gravity(TreeGravArgs a) 
   const float eps2 = a.eps2;
   const double theta = a.theta;
   double ax = 0, ay = 0, az = 0, ap = 0;
-  int nlist = 0, nruns = 0;
+  int nlist = 0;
+  unsigned head = 0, tail = 0;  // ring positions (mod kTgRing)
   bool ok = true;
 
   const f32x2 X2 = pk2(xi, xi), Y2 = pk2(yi, yi), Z2 = pk2(zi, zi), E2 = pk2(eps2, eps2);
@@ -235,7 +274,7 @@ __global__ void __launch_bounds__(kTgWarps * 32) k_tree_gravity(TreeGravArgs a) 
       const f32x2 qy = fma2(qyz, rz, fma2(qyy, ry, mul2(qxy, rx)));
       const f32x2 qz = fma2(qzz, rz, fma2(qyz, ry, mul2(qxz, rx)));
       const f32x2 rqr = fma2(rz, qz, fma2(ry, qy, mul2(rx, qx)));
-      const f32x2 t = mul2(rqr, inv5);                          // (r.Q.r) / s^5
+      const f32x2 t = mul2(rqr, inv5);                             // (r.Q.r) / s^5
       const f32x2 c = fma2(HALF5, mul2(t, inv2), mul2(em, inv3));  // M / s^3 + (5/2) (r.Q.r) / s^7
       const f32x2 ni5 = mul2(inv5, MONE);
       px = fma2(ni5, qx, fma2(c, rx, px));
@@ -251,91 +290,91 @@ __global__ void __launch_bounds__(kTgWarps * 32) k_tree_gravity(TreeGravArgs a) 
     nlist = 0;
     __syncwarp();  // every lane is done reading before the list is refilled
   };
-  // sweep the buffered level-0 runs, 32 source particles at a time
-  auto sweep_runs = [&]() {
+  // sweep 32 ring entries from `head` (fewer at the end: the rest padded far away and massless)
+  auto sweep_chunk = [&](unsigned cnt) {
     __syncwarp();
-    for (int r0 = 0; r0 < nruns; r0 += 4) {
-      const int r = r0 + (int)(lane >> 3);
-      float4 q = make_float4(1e18f, 1e18f, 1e18f, 0.f);  // padding: far away, massless
-      if (r < nruns) {
-        const int sj = sm.runs[r] * kGFan + (int)(lane & 7u);
-        if (sj < n) {
-          const double4 p = a.src[sj];
-          q = make_float4((float)(p.x - anc.x), (float)(p.y - anc.y), (float)(p.z - anc.z), (float)p.w);
-        }
-      }
-      __syncwarp();
-      sm.part[lane] = q;
-      __syncwarp();
-      float px = 0.f, py = 0.f, pz = 0.f, pp = 0.f;
-#pragma unroll 8
-      for (int k = 0; k < 32; k++) {
-        const float4 p = sm.part[k];
-        const float dx = p.x - xi, dy = p.y - yi, dz = p.z - zi;
-        const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
-        const float inv = rsqrt_f32(r2);
-        const float sj = p.w * inv;
-        const float s3 = sj * inv * inv;
-        px = fmaf(dx, s3, px);
-        py = fmaf(dy, s3, py);
-        pz = fmaf(dz, s3, pz);
-        pp -= sj;
-      }
-      ax += px; ay += py; az += pz; ap += pp;
+    float4 q = make_float4(1e18f, 1e18f, 1e18f, 0.f);
+    if (lane < cnt) {
+      const double4 p = a.src[sm.ring[(head + lane) % kTgRing]];
+      q = make_float4((float)(p.x - anc.x), (float)(p.y - anc.y), (float)(p.z - anc.z), (float)p.w);
     }
-    nruns = 0;
+    sm.part[lane] = q;
+    __syncwarp();
+    float px = 0.f, py = 0.f, pz = 0.f, pp = 0.f;
+#pragma unroll 8
+    for (int k = 0; k < 32; k++) {
+      const float4 p = sm.part[k];
+      const float dx = p.x - xi, dy = p.y - yi, dz = p.z - zi;
+      const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
+      const float inv = rsqrt_f32(r2);
+      const float sj = p.w * inv;
+      const float s3 = sj * inv * inv;
+      px = fmaf(dx, s3, px);
+      py = fmaf(dy, s3, py);
+      pz = fmaf(dz, s3, pz);
+      pp -= sj;
+    }
+    ax += px; ay += py; az += pz; ap += pp;
+    head += cnt;
     __syncwarp();
   };
 
-  const int top = a.g.levels - 1;
-  int sp = 1;
-  if (lane == 0) sm.stack[0] = (top << 26);  // the root
+  int sp = 0;
+  if (n < 2) {  // a single particle: no internal node
+    if (lane == 0) sm.ring[0] = 0;
+    tail = 1;
+  } else {
+    if (lane == 0) sm.stack[0] = 0;  // the root covers [0, n)
+    sp = 1;
+  }
   __syncwarp();
-  // the root itself is tested like any child: pretend its parent is popped
-  bool root_round = true;
   while (sp > 0) {
-    // pop up to four nodes; lane L tests child (L & 7) of popped node (L >> 3)
-    const int take = min(sp, 4);
-    const int slot = (int)(lane >> 3);
-    int e = 0;
-    if (slot < take) e = sm.stack[sp - 1 - slot];
+    // pop up to sixteen nodes; lane L tests child (L & 1) of popped node (L >> 1)
+    const int take = min(sp, 16);
+    const int slot = (int)(lane >> 1);
+    int node = -1;
+    if (slot < take) node = sm.stack[sp - 1 - slot];
     sp -= take;
     __syncwarp();
-    const int plevel = e >> 26, pnode = e & ((1 << 26) - 1);
-    int level, child;
-    bool exists;
-    if (root_round) {  // the root: lane 0 only
-      level = top;
-      child = 0;
-      exists = lane == 0;
-      root_round = false;
-    } else {
-      level = plevel - 1;
-      child = pnode * kGFan + (int)(lane & 7u);
-      exists = slot < take && child < a.g.count[level];
+    int ref = 0;
+    bool live = slot < take;
+    if (live) {
+      const int2 ch = a.w.child[node];
+      ref = (lane & 1u) ? ch.y : ch.x;
     }
-    bool accept = false;
+    bool accept = false, open = false;
+    int p0 = 0, pc = 0;  // source particles this lane hands to the ring
     double4 c = make_double4(0, 0, 0, 0);
-    if (exists) {
-      const long long k = a.g.base[level] + child;
-      c = a.cm[k];
-      const double b = a.q1[k].z;
-      exists = c.w > 0;
-      const double ddx = fmax(fmax((double)gl.x - c.x, c.x - (double)gh.x), 0.0);
-      const double ddy = fmax(fmax((double)gl.y - c.y, c.y - (double)gh.y), 0.0);
-      const double ddz = fmax(fmax((double)gl.z - c.z, c.z - (double)gh.z), 0.0);
-      accept = exists && b < theta * sqrt(ddx * ddx + ddy * ddy + ddz * ddz);
+    if (live && ref < 0) {
+      p0 = ~ref;
+      pc = 1;
+    } else if (live) {
+      c = a.w.cm[ref];
+      const double4 qb = a.w.q1[ref];
+      if (c.w > 0) {
+        const double ddx = fmax(fmax((double)gl.x - c.x, c.x - (double)gh.x), 0.0);
+        const double ddy = fmax(fmax((double)gl.y - c.y, c.y - (double)gh.y), 0.0);
+        const double ddz = fmax(fmax((double)gl.z - c.z, c.z - (double)gh.z), 0.0);
+        accept = qb.z < theta * sqrt(ddx * ddx + ddy * ddy + ddz * ddz);
+        if (!accept) {
+          if (qb.w <= (double)kBucket) {
+            p0 = a.w.range[ref].x;
+            pc = (int)qb.w;
+          } else {
+            open = true;
+          }
+        }
+      }
     }
     // accepted nodes -> the list (swept first when it could overflow)
     const unsigned am = __ballot_sync(0xffffffffu, accept);
     if (am) {
       if (nlist + __popc(am) > kTgList) sweep_list();
       if (accept) {
-        const long long k = a.g.base[level] + child;
-        const double4 qa = a.q0[k], qb = a.q1[k];
-        const int slot = nlist + __popc(am & ((1u << lane) - 1u));
-        NodePair &e = sm.list[slot >> 1];
-        const int h = slot & 1;
+        const double4 qa = a.w.q0[ref], qb = a.w.q1[ref];
+        const int k = nlist + __popc(am & ((1u << lane) - 1u));
+        NodePair &e = sm.list[k >> 1];
+        const int h = k & 1;
         e.x[h] = (float)(c.x - anc.x); e.y[h] = (float)(c.y - anc.y); e.z[h] = (float)(c.z - anc.z);
         e.m[h] = (float)c.w;
         e.qxx[h] = (float)qa.x; e.qyy[h] = (float)qa.y; e.qzz[h] = (float)qa.z; e.qxy[h] = (float)qa.w;
@@ -344,46 +383,58 @@ __global__ void __launch_bounds__(kTgWarps * 32) k_tree_gravity(TreeGravArgs a) 
       nlist += __popc(am);
       __syncwarp();
     }
-    const bool open = exists && !accept;
-    // opened level-0 nodes -> the run buffer
-    const unsigned rm = __ballot_sync(0xffffffffu, open && level == 0);
-    if (rm) {
-      if (nruns + __popc(rm) > kTgRuns) sweep_runs();
-      if (open && level == 0) sm.runs[nruns + __popc(rm & ((1u << lane) - 1u))] = child;
-      nruns += __popc(rm);
-      __syncwarp();
+    // particles -> the ring (warp prefix sum of the counts), then every full chunk is swept
+    int incl = pc;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if ((int)lane >= o) incl += v;
     }
-    // opened higher nodes -> the stack
-    const unsigned om = __ballot_sync(0xffffffffu, open && level > 0);
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    if (total > 0) {
+      for (int k = 0; k < pc; k++) sm.ring[(tail + (unsigned)(incl - pc + k)) % kTgRing] = p0 + k;
+      tail += (unsigned)total;
+      while (tail - head >= 32u) sweep_chunk(32u);
+    }
+    // opened larger nodes -> the stack
+    const unsigned om = __ballot_sync(0xffffffffu, open);
     const int cnt = __popc(om);
     if (sp + cnt > kTgStack) {
       ok = false;
       break;
     }
-    if (open && level > 0) sm.stack[sp + cnt - 1 - __popc(om & ((1u << lane) - 1u))] = (level << 26) | child;
+    if (open) sm.stack[sp + cnt - 1 - __popc(om & ((1u << lane) - 1u))] = ref;
     sp += cnt;
     __syncwarp();
   }
   __syncwarp();
   if (nlist > 0) sweep_list();
-  if (nruns > 0) sweep_runs();
+  if (tail != head) sweep_chunk(tail - head);
   if (!ok && lane == 0) raise_flag(a.flags, SPH_FLAG_STACK_OVERFLOW);
   if (valid) a.out[s] = make_double4(a.G * ax, a.G * ay, a.G * az, a.G * ap);
 }
 
-// Shard `rank` of `world` computes the groups of its leaf range into `out`,
-// zeroed first when world > 1 (the sum over shards is the whole field).
-int launch_tree_gravity(const TreeView &t, const double4 *src, double4 *cm, double4 *q0, double4 *q1, double4 *out,
+// keys: the sorted Morton keys of the current particle order (the sort's
+// output); ws: tree_gravity_workspace_bytes(n) bytes.  Shard `rank` of
+// `world` computes the groups of its leaf range into `out`, zeroed first
+// when world > 1 (the sum over shards is the whole field).
+int launch_tree_gravity(const TreeView &t, const uint64_t *keys, const double4 *src, void *ws, double4 *out,
                         unsigned *flags, double eps, double theta, double G, int rank, int world, cudaStream_t st) {
-  if (t.n <= 0) return 0;
-  const GTree g = gtree_layout(t.n);
-  int launches = gtree_moments(g, t.n, src, cm, q0, q1, st);
-  if (world > 1) cudaMemsetAsync(out, 0, sizeof(double4) * t.n, st);
+  const int n = t.n;
+  if (n <= 0) return 0;
+  const TgWork w = carve(ws, n);
+  int launches = 0;
+  if (n > 1) {
+    k_radix_tree<<<(n - 1 + 255) / 256, 256, 0, st>>>(n, keys, w);
+    k_tree_moments<<<(n + 255) / 256, 256, 0, st>>>(n, src, w);
+    launches += 2;
+  }
+  if (world > 1) cudaMemsetAsync(out, 0, sizeof(double4) * n, st);
   long long l0, l1;
   shard_range(t.count[0], rank, world, l0, l1);
   if (l1 <= l0) return launches;
   TreeGravArgs a;
-  a.t = t; a.g = g; a.src = src; a.cm = cm; a.q0 = q0; a.q1 = q1; a.out = out; a.flags = flags;
+  a.t = t; a.w = w; a.src = src; a.out = out; a.flags = flags;
   a.eps2 = (float)(eps * eps); a.theta = (float)theta; a.G = G;
   a.leaf0 = (int)l0; a.leaf1 = (int)l1;
   const int warps = (int)(l1 - l0);
