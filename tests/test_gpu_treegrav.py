@@ -16,7 +16,7 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 # RMS force error bounds per opening angle (measured on the N = 20,000
-# polytrope with eps = 0.01: 4.8e-8, 4.3e-5, 2.4e-4, 6.9e-4)
+# polytrope with eps = 0.01: 4.8e-8, 2.4e-5, 1.4e-4, 4.9e-4)
 BOUNDS = {0.0: 1e-6, 0.3: 1e-4, 0.5: 1e-3, 0.7: 3e-3}
 
 
