@@ -42,6 +42,7 @@ class Params(C.Structure):
         ("soft_mode", C.c_int), ("eps", C.c_double), ("use_psi", C.c_int), ("cn1", C.c_double),
         ("cn2", C.c_double), ("G", C.c_double), ("precision", C.c_int), ("ngb_cap", C.c_int),
         ("sort_every", C.c_int), ("mixed_sph", C.c_int), ("grav_mode", C.c_int), ("theta", C.c_double),
+        ("key_mode", C.c_int),
     ]
 
 
@@ -87,6 +88,8 @@ def lib():
     L.cudasph_sort_scratch_bytes.argtypes = [ip]
     L.cudasph_sort_scratch_bytes.restype = C.c_size_t
     L.cudasph_morton_keys.argtypes = [ip, vp, vp, vp, vp, vp, vp]
+    L.cudasph_peano_keys.argtypes = [ip, vp, vp, vp, vp, vp, vp]
+    L.cudasph_peano_hilbert_keys.argtypes = [ip, vp, vp, vp, ip, vp, vp]
     L.cudasph_radix_sort_u64.argtypes = [ip, vp, vp, vp, vp]
     L.cudasph_gravity_direct.argtypes = [ip, vp, vp, vp, ip, dp, dp, ip, vp]
     L.cudasph_fma_peak.argtypes = [ip, ip, vp]

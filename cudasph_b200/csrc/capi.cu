@@ -19,6 +19,8 @@ size_t radix_scratch_bytes(int n);
 int radix_sort_u64(int n, uint64_t *keys, uint32_t *vals, void *scratch, cudaStream_t st);
 int morton_keys(int n, const double4 *pos, const double *x, const double *y, const double *z, double *part,
                 double *box4, uint64_t *keys, uint32_t *vals, cudaStream_t st);
+int peano_keys(int n, const double4 *pos, const double *x, const double *y, const double *z, double *part,
+               double *box4, uint64_t *keys, uint32_t *vals, cudaStream_t st);
 int tree_layout(int n, TreeView *t);
 int build_tree(const TreeView &t, const double4 *pos, float4 *lo, float4 *hi, cudaStream_t st);
 int launch_solve_range(const TreeView &t, double4 *pos, int *nevals, unsigned *flags, const sph_params &p,
@@ -201,6 +203,7 @@ int check_params(const sph_params *p) {
   if (p->ngb_cap < 0 || p->sort_every < 0 || p->mixed_sph < 0 || p->mixed_sph > 3) return SPH_ERR_ARG;
   if (!(p->gamma > 1)) return SPH_ERR_ARG;
   if (p->grav_mode != SPH_GRAV_DIRECT && p->grav_mode != SPH_GRAV_TREE) return SPH_ERR_ARG;
+  if (p->key_mode != SPH_KEY_MORTON && p->key_mode != SPH_KEY_PEANO) return SPH_ERR_ARG;
   if (p->grav_mode == SPH_GRAV_TREE && (p->soft_mode != SPH_SOFT_PLUMMER || !(p->theta >= 0) || !(p->theta < 1)))
     return SPH_ERR_ARG;
   return SPH_OK;
@@ -276,6 +279,7 @@ extern "C" sph_params cudasph_default_params(void) {
   p.mixed_sph = 0;
   p.grav_mode = SPH_GRAV_DIRECT;
   p.theta = 0.5;
+  p.key_mode = SPH_KEY_MORTON;
   return p;
 }
 
@@ -573,7 +577,10 @@ extern "C" int cudasph_sort(sph_ctx *c) {
   const int n = c->n;
   Fields &S = c->f[c->cur];
   Fields &D = c->f[1 - c->cur];
-  LAUNCHED(morton_keys(n, S.pos, nullptr, nullptr, nullptr, c->bbox_part, c->box4, c->keys, c->vals, c->st));
+  if (c->p.key_mode == SPH_KEY_PEANO)
+    LAUNCHED(peano_keys(n, S.pos, nullptr, nullptr, nullptr, c->bbox_part, c->box4, c->keys, c->vals, c->st));
+  else
+    LAUNCHED(morton_keys(n, S.pos, nullptr, nullptr, nullptr, c->bbox_part, c->box4, c->keys, c->vals, c->st));
   LAUNCHED(radix_sort_u64(n, c->keys, c->vals, c->sort_scratch, c->st));
   LAUNCHED(launch_permute(n, c->vals, S, D, c->st));
   c->cur = 1 - c->cur;

@@ -1,5 +1,6 @@
 // sort.cu -- Morton keys and a stable LSD radix sort (the space-filling-curve
-// sort of sort_bodies.cpp:119-186, done on the device every step).
+// sort of sort_bodies.cpp:119-186, done on the device every step), and the
+// reference's Peano-Hilbert keys as an optional sort key.
 //
 // Keys: positions quantised to 21 bits per dimension in the bounding cube
 // (scale = 2^21 / max extent, like domain_fac of sort_bodies.cpp:135), bits
@@ -246,6 +247,192 @@ int morton_keys(int n, const double4 *pos, const double *x, const double *y, con
 }
 
 // ---------------------------------------------------------------------------
+// Peano-Hilbert keys: the reference's space-filling curve (sort_bodies.cpp:
+// 66-105), an optional sort key (sph_params.key_mode) for the reference's
+// particle order.  Each level of a key descends into one octant of the
+// current cell; the octant's rank along the curve is the level's 3-bit
+// digit, and the octant's sub-cells are visited in a rotated frame, possibly
+// in reverse.  Frames are proper rotations of the cube.  The curve is fixed
+// by
+//   * the visiting order in the unrotated frame: rank q visits the octant
+//     whose (z, x, y) bits are the Gray code q ^ (q >> 1);
+//   * per rank q, the child's frame: the parent's frame followed by
+//     kPhTurnsX[q] quarter turns about x and kPhTurnsY[q] about y, and
+//     whether the child's direction is the reverse of its parent's.
+// Those per-rank turns and reversals carry the same information as
+// rotx_table, roty_table and sense_table (sort_bodies.cpp:53-57): the keys
+// agree only for the same curve.  The (frame, direction) pairs reachable
+// from the root form a 24-state automaton, generated at compile time, so a
+// key costs one shared-memory lookup per level: entry = next state * 8 +
+// digit, indexed by state * 8 + (bx << 2 | by << 1 | bz).
+// ---------------------------------------------------------------------------
+struct PhFrame {
+  int m[9];  // row-major signed permutation matrix
+};
+
+constexpr PhFrame ph_mul(const PhFrame &a, const PhFrame &b) {
+  PhFrame r{};
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      int v = 0;
+      for (int k = 0; k < 3; k++) v += a.m[i * 3 + k] * b.m[k * 3 + j];
+      r.m[i * 3 + j] = v;
+    }
+  return r;
+}
+
+constexpr bool ph_same(const PhFrame &a, const PhFrame &b) {
+  for (int i = 0; i < 9; i++)
+    if (a.m[i] != b.m[i]) return false;
+  return true;
+}
+
+constexpr PhFrame kPhTurnX = {{1, 0, 0, 0, 0, 1, 0, -1, 0}};  // quarter turn about x
+constexpr PhFrame kPhTurnY = {{0, 0, -1, 0, 1, 0, 1, 0, 0}};  // quarter turn about y
+constexpr int kPhTurnsX[8] = {3, 0, 0, 2, 2, 0, 0, 1};
+constexpr int kPhTurnsY[8] = {0, 1, 1, 2, 2, 3, 3, 0};
+constexpr int kPhReverse[8] = {1, 1, 1, 0, 0, 1, 1, 1};
+constexpr int kPhStates = 24;
+constexpr int kPhMaxStates = 48;  // frames x directions
+
+constexpr int ph_gray_rank(int g) {
+  int q = 0;
+  for (; g; g >>= 1) q ^= g;
+  return q;
+}
+
+// rank along the curve, in frame f, of the world octant o = bx << 2 | by << 1 | bz
+constexpr int ph_rank(const PhFrame &f, int o) {
+  const int s[3] = {((o >> 2) & 1) * 2 - 1, ((o >> 1) & 1) * 2 - 1, (o & 1) * 2 - 1};
+  int l[3] = {0, 0, 0};  // the octant's centre in the frame's own axes: f^T s
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) l[i] += f.m[j * 3 + i] * s[j];
+  const int bx = (l[0] + 1) / 2, by = (l[1] + 1) / 2, bz = (l[2] + 1) / 2;
+  return ph_gray_rank((bz << 2) | (bx << 1) | by);
+}
+
+struct PhTable {
+  uint16_t e[kPhMaxStates * 8];
+  int nstates;
+};
+
+constexpr PhTable make_ph_table() {
+  PhFrame frame[kPhMaxStates] = {};
+  int rev[kPhMaxStates] = {};
+  frame[0] = PhFrame{{1, 0, 0, 0, 1, 0, 0, 0, 1}};
+  int ns = 1;
+  PhTable t{};
+  for (int s = 0; s < ns; s++)
+    for (int o = 0; o < 8; o++) {
+      const int q = ph_rank(frame[s], o);
+      PhFrame f = frame[s];
+      for (int k = 0; k < kPhTurnsX[q]; k++) f = ph_mul(f, kPhTurnX);
+      for (int k = 0; k < kPhTurnsY[q]; k++) f = ph_mul(f, kPhTurnY);
+      const int r = rev[s] ^ kPhReverse[q];
+      int id = 0;
+      while (id < ns && !(rev[id] == r && ph_same(frame[id], f))) id++;
+      if (id == ns) {  // a new state (at most kPhMaxStates exist)
+        frame[ns] = f;
+        rev[ns] = r;
+        ns++;
+      }
+      t.e[s * 8 + o] = (uint16_t)(id * 8 + (rev[s] ? 7 - q : q));
+    }
+  t.nstates = ns;
+  return t;
+}
+
+static_assert(make_ph_table().nstates == kPhStates, "the curve's automaton has 24 states");
+
+__constant__ PhTable g_ph_table = make_ph_table();
+
+__device__ __forceinline__ void ph_load_table(uint16_t *tab) {
+  for (int i = threadIdx.x; i < kPhStates * 8; i += blockDim.x) tab[i] = g_ph_table.e[i];
+  __syncthreads();
+}
+
+// key of the integer triplet: levels bits-1 .. 0 of each coordinate (higher
+// bits are ignored, as the reference's mask does)
+__device__ __forceinline__ uint64_t ph_key(const uint16_t *tab, uint32_t x, uint32_t y, uint32_t z, int bits) {
+  uint64_t key = 0;
+  int s = 0;  // state * 8
+  for (int l = bits - 1; l >= 0; l--) {
+    const int o = (((x >> l) & 1u) << 2) | (((y >> l) & 1u) << 1) | ((z >> l) & 1u);
+    const int e = tab[s + o];
+    key = (key << 3) | (uint64_t)(e & 7);
+    s = e & ~7;
+  }
+  return key;
+}
+
+__global__ void k_peano_int(int n, const int *__restrict__ x, const int *__restrict__ y, const int *__restrict__ z,
+                            int bits, uint64_t *__restrict__ keys) {
+  __shared__ uint16_t tab[kPhStates * 8];
+  ph_load_table(tab);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    keys[i] = ph_key(tab, (uint32_t)x[i], (uint32_t)y[i], (uint32_t)z[i], bits);
+}
+
+constexpr int kPhBits = 18;  // BITS_PER_DIMENSION, sort_bodies.cpp:3
+
+// the reference's quantisation box (sort_bodies.cpp:121-135) in float, from
+// the double bounding box (rounding is monotone, so the float box of the
+// float-rounded positions is the rounded double box): box4 = {lo.x, lo.y,
+// lo.z, domain_fac}, domain_fac = float(1.0 / size * 2^18) with size the
+// largest float extent; 0 for a degenerate box (all keys 0)
+__global__ void k_peano_box_final(int nb, const double *__restrict__ part, double *__restrict__ box4) {
+  if (threadIdx.x != 0) return;
+  double lo[3] = {1e308, 1e308, 1e308}, hi[3] = {-1e308, -1e308, -1e308};
+  for (int b = 0; b < nb; b++)
+    for (int d = 0; d < 3; d++) { lo[d] = fmin(lo[d], part[b * 6 + d]); hi[d] = fmax(hi[d], part[b * 6 + 3 + d]); }
+  float lf[3], ext[3];
+  for (int d = 0; d < 3; d++) {
+    lf[d] = __double2float_rn(lo[d]);
+    ext[d] = __fsub_rn(__double2float_rn(hi[d]), lf[d]);
+  }
+  const float size = fmaxf(ext[2], fmaxf(ext[1], ext[0]));
+  const float fac = size > 0.f ? __double2float_rn(__dmul_rn(__ddiv_rn(1.0, (double)size), (double)(1 << kPhBits)))
+                               : 0.f;
+  box4[0] = lf[0]; box4[1] = lf[1]; box4[2] = lf[2]; box4[3] = fac;
+}
+
+// positions rounded to float (the reference's float4 state), offset and
+// scaled in float and truncated (sort_bodies.cpp:155-159), then keyed
+__global__ void k_peano_pos(int n, const double4 *__restrict__ pos, const double *__restrict__ x,
+                            const double *__restrict__ y, const double *__restrict__ z,
+                            const double *__restrict__ box4, uint64_t *__restrict__ keys, uint32_t *__restrict__ vals) {
+  __shared__ uint16_t tab[kPhStates * 8];
+  ph_load_table(tab);
+  const float lx = (float)box4[0], ly = (float)box4[1], lz = (float)box4[2], fac = (float)box4[3];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double c0, c1, c2;
+    if (pos) {
+      const double4 p = pos[i];
+      c0 = p.x; c1 = p.y; c2 = p.z;
+    } else {
+      c0 = x[i]; c1 = y[i]; c2 = z[i];
+    }
+    const int qx = __float2int_rz(__fmul_rn(__fsub_rn(__double2float_rn(c0), lx), fac));
+    const int qy = __float2int_rz(__fmul_rn(__fsub_rn(__double2float_rn(c1), ly), fac));
+    const int qz = __float2int_rz(__fmul_rn(__fsub_rn(__double2float_rn(c2), lz), fac));
+    keys[i] = ph_key(tab, (uint32_t)qx, (uint32_t)qy, (uint32_t)qz, kPhBits);
+    if (vals) vals[i] = (uint32_t)i;
+  }
+}
+
+// bounding box + Peano-Hilbert keys of positions (double4 records or x/y/z)
+int peano_keys(int n, const double4 *pos, const double *x, const double *y, const double *z, double *part,
+               double *box4, uint64_t *keys, uint32_t *vals, cudaStream_t st) {
+  int nb = 148 * 2;
+  if (nb * 256 > n) nb = (n + 255) / 256;
+  if (nb < 1) nb = 1;
+  k_bbox_partial<<<nb, 256, 0, st>>>(n, pos, x, y, z, part);
+  k_peano_box_final<<<1, 32, 0, st>>>(nb, part, box4);
+  k_peano_pos<<<(n + 255) / 256, 256, 0, st>>>(n, pos, x, y, z, box4, keys, vals);
+  return 3;
+}
+
+// ---------------------------------------------------------------------------
 // Allocation-free variant of the radix sort.  Its scratch (ping-pong key and
 // value buffers plus the per-block digit histograms) is a file-scope device
 // array sized for kNoAllocMaxKeys keys; every GPU that loads this library
@@ -313,6 +500,30 @@ extern "C" size_t cudasph_sort_scratch_bytes(int n) { return sph::radix_scratch_
 extern "C" int cudasph_radix_sort_u64(int n, uint64_t *keys, uint32_t *vals, void *scratch, void *stream) {
   if (n < 0 || (n > 0 && (!keys || !vals || !scratch))) return SPH_ERR_ARG;
   sph::radix_sort_u64(n, keys, vals, scratch, (cudaStream_t)stream);
+  SPH_CUDA_TRY(cudaGetLastError());
+  return SPH_OK;
+}
+
+extern "C" int cudasph_peano_keys(int n, const double *x, const double *y, const double *z, uint64_t *keys,
+                                  double *box4, void *stream) {
+  if (n <= 0) return n == 0 ? SPH_OK : SPH_ERR_ARG;
+  if (!x || !y || !z || !keys || !box4) return SPH_ERR_ARG;
+  double *part = nullptr;
+  SPH_CUDA_TRY(cudaMallocAsync((void **)&part, 148 * 2 * 6 * sizeof(double), (cudaStream_t)stream));
+  sph::peano_keys(n, nullptr, x, y, z, part, box4, keys, nullptr, (cudaStream_t)stream);
+  SPH_CUDA_TRY(cudaFreeAsync(part, (cudaStream_t)stream));
+  SPH_CUDA_TRY(cudaGetLastError());
+  return SPH_OK;
+}
+
+extern "C" int cudasph_peano_hilbert_keys(int n, const int *x, const int *y, const int *z, int bits, uint64_t *keys,
+                                          void *stream) {
+  if (n < 0 || bits < 1 || bits > 21) return SPH_ERR_ARG;
+  if (n == 0) return SPH_OK;
+  if (!x || !y || !z || !keys) return SPH_ERR_ARG;
+  int nb = (n + 255) / 256;
+  if (nb > 148 * 8) nb = 148 * 8;
+  sph::k_peano_int<<<nb, 256, 0, (cudaStream_t)stream>>>(n, x, y, z, bits, keys);
   SPH_CUDA_TRY(cudaGetLastError());
   return SPH_OK;
 }

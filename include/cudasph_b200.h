@@ -55,6 +55,7 @@ typedef enum { SPH_EOS_IDEAL = 0, SPH_EOS_GAS_RADIATION = 1 } sph_eos_mode;
 typedef enum { SPH_SOFT_SPLINE = 0, SPH_SOFT_PLUMMER = 1 } sph_soft_mode;
 typedef enum { SPH_PREC_FP64 = 0, SPH_PREC_MIXED = 1 } sph_precision;
 typedef enum { SPH_GRAV_DIRECT = 0, SPH_GRAV_TREE = 1 } sph_grav_mode;
+typedef enum { SPH_KEY_MORTON = 0, SPH_KEY_PEANO = 1 } sph_key_mode;
 
 typedef struct {
   double n_target;   /* smoothed neighbour number; DESIRED_NGB, dev_solve_range.cu:14 */
@@ -84,6 +85,10 @@ typedef struct {
                         Plummer softening only; force error set by theta) */
   double theta;      /* tree opening angle: a node of radius b is accepted when b < theta * its
                         distance to the target group's box (default 0.5) */
+  int key_mode;      /* sph_key_mode of the spatial sort: Morton keys, 21 bits per dimension in
+                        the double bounding cube (default), or the reference's Peano-Hilbert keys
+                        (sort_bodies.cpp:66-160: positions rounded to float, 18 bits per
+                        dimension), which reproduce its particle order */
 } sph_params;
 
 /* particle fields, addressed in the caller's ORIGINAL particle order */
@@ -259,6 +264,21 @@ size_t cudasph_sort_scratch_bytes(int n);
 int cudasph_morton_keys(int n, const double *x, const double *y, const double *z, uint64_t *keys,
                         double *box4 /* device, 4 doubles: lo xyz, scale */, void *stream);
 int cudasph_radix_sort_u64(int n, uint64_t *keys, uint32_t *vals, void *scratch, void *stream);
+
+/* Peano-Hilbert keys of the reference's curve.  cudasph_peano_hilbert_keys is
+ * peano_hilbert_key(x, y, z, bits) of sort_bodies.cpp:66-105 over n integer
+ * triplets (device arrays; bits in [1, 21]; coordinate bits above bits-1 are
+ * ignored).  cudasph_peano_keys keys positions the way CUDAsph::sort_bodies
+ * does (sort_bodies.cpp:121-160): coordinates rounded to float, offset by the
+ * float bounding box's low corner, scaled by domain_fac = float(2^18 / largest
+ * extent) in float and truncated, 18 bits per dimension (a coordinate at the
+ * box's far side becomes 2^18 and keeps its low 18 bits, as there); box4
+ * receives {lo.x, lo.y, lo.z, domain_fac}.  A degenerate box (one point) gives
+ * domain_fac = 0 and all keys 0. */
+int cudasph_peano_hilbert_keys(int n, const int *x, const int *y, const int *z, int bits, uint64_t *keys,
+                               void *stream);
+int cudasph_peano_keys(int n, const double *x, const double *y, const double *z, uint64_t *keys,
+                       double *box4 /* device, 4 doubles */, void *stream);
 
 /* Allocation-free variant of cudasph_radix_sort_u64; it has no counterpart
  * in the reference.  It is for callers that cannot allocate device memory on

@@ -82,6 +82,9 @@ def lib():
     L.orc_hydro.argtypes = [C.c_int] + [_dp] * 14 + [_lp, _ip] + [_dp] * 5 + [C.c_void_p, C.POINTER(OrcParams)]
     L.orc_gravity.argtypes = [C.c_int, C.c_void_p, C.c_int] + [_dp] * 9 + [C.POINTER(OrcParams)]
     L.orc_morton_keys.argtypes = [C.c_int, _dp, _dp, _dp, _up, C.c_void_p]
+    L.orc_peano_keys.argtypes = [C.c_int, _dp, _dp, _dp, _up, C.c_void_p]
+    L.orc_peano_hilbert_key.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int]
+    L.orc_peano_hilbert_key.restype = C.c_uint64
     L.orc_sort_order.argtypes = [C.c_int, _up, _ip]
     L.orc_timestep.argtypes = [C.c_int, _dp, _dp, _dp, _dp, C.POINTER(OrcParams)]
     L.orc_timestep.restype = C.c_double
@@ -182,6 +185,21 @@ def morton_keys(x, y, z):
     box = np.zeros(4)
     lib().orc_morton_keys(x.size, x, y, z, k, box.ctypes.data_as(C.c_void_p))
     return k, box
+
+
+def peano_keys(x, y, z):
+    """Peano-Hilbert keys of positions as CUDAsph::sort_bodies makes them
+    (sort_bodies.cpp:121-160, float quantisation, 18 bits per dimension)."""
+    x, y, z = _f64(x), _f64(y), _f64(z)
+    k = np.zeros(x.size, np.uint64)
+    box = np.zeros(4)
+    lib().orc_peano_keys(x.size, x, y, z, k, box.ctypes.data_as(C.c_void_p))
+    return k, box
+
+
+def peano_hilbert_key(x, y, z, bits):
+    """peano_hilbert_key of one integer triplet (sort_bodies.cpp:66-105)."""
+    return int(lib().orc_peano_hilbert_key(int(x), int(y), int(z), int(bits)))
 
 
 def sort_order(keys):

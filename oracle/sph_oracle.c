@@ -728,6 +728,83 @@ void orc_morton_keys(int n, const double *x, const double *y, const double *z, u
   }
 }
 
+/* ------------------------------------------------------------------ */
+/* Peano-Hilbert keys: peano_hilbert_key sort_bodies.cpp:66-105 and the  */
+/* float quantisation of CUDAsph::sort_bodies sort_bodies.cpp:121-160.   */
+/* ------------------------------------------------------------------ */
+/* The curve, level by level: the current cell is traversed in a frame f (a
+   proper rotation of the cube) and a direction.  The world octant
+   (bx, by, bz) has the frame-local octant f^T (2b - 1); its rank q along the
+   curve is the inverse Gray code of the local (z, x, y) bits, and the key
+   digit is q, or 7 - q in a reversed direction (sort_bodies.cpp:84-85).  The
+   child's frame is f followed by TX[q] quarter turns about x and TY[q] about
+   y (the rotations applied by rotxmap_table / rotymap_table,
+   sort_bodies.cpp:87-101); the child's direction flips where REV[q] (the
+   sense_table sign, :89). */
+static const int PH_TX[8] = {3, 0, 0, 2, 2, 0, 0, 1};
+static const int PH_TY[8] = {0, 1, 1, 2, 2, 3, 3, 0};
+static const int PH_REV[8] = {1, 1, 1, 0, 0, 1, 1, 1};
+
+static void mat3_mul(const int *a, const int *b, int *r) {
+  int t[9];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      int v = 0;
+      for (int k = 0; k < 3; k++) v += a[i * 3 + k] * b[k * 3 + j];
+      t[i * 3 + j] = v;
+    }
+  memcpy(r, t, sizeof(t));
+}
+
+uint64_t orc_peano_hilbert_key(int x, int y, int z, int bits) {
+  static const int turn_x[9] = {1, 0, 0, 0, 0, 1, 0, -1, 0};
+  static const int turn_y[9] = {0, 0, -1, 0, 1, 0, 1, 0, 0};
+  int f[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  int rev = 0;
+  uint64_t key = 0;
+  for (int l = bits - 1; l >= 0; l--) {
+    const int s[3] = {((x >> l) & 1) * 2 - 1, ((y >> l) & 1) * 2 - 1, ((z >> l) & 1) * 2 - 1};
+    int loc[3] = {0, 0, 0};
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) loc[i] += f[j * 3 + i] * s[j];
+    int g = (((loc[2] + 1) / 2) << 2) | (((loc[0] + 1) / 2) << 1) | ((loc[1] + 1) / 2);
+    int q = 0;
+    for (; g; g >>= 1) q ^= g;
+    key = (key << 3) | (uint64_t)(rev ? 7 - q : q);
+    for (int k = 0; k < PH_TX[q]; k++) mat3_mul(f, turn_x, f);
+    for (int k = 0; k < PH_TY[q]; k++) mat3_mul(f, turn_y, f);
+    rev ^= PH_REV[q];
+  }
+  return key;
+}
+
+/* keys of positions as sort_bodies.cpp:121-160 computes them on its float4
+   state: float bounding box, domain_fac = float(1.0 / size * 2^18), then
+   (int)((pos - r_min) * domain_fac) in float, 18 bits per dimension.  box =
+   {r_min.x, r_min.y, r_min.z, domain_fac}; a degenerate box (size 0) gives
+   domain_fac = 0 (the reference divides by zero there). */
+void orc_peano_keys(int n, const double *x, const double *y, const double *z, uint64_t *keys, double *box) {
+  if (n <= 0) return;
+  float lo[3] = {(float)x[0], (float)y[0], (float)z[0]}, hi[3] = {lo[0], lo[1], lo[2]};
+  for (int i = 1; i < n; i++) {
+    const float c[3] = {(float)x[i], (float)y[i], (float)z[i]};
+    for (int d = 0; d < 3; d++) {
+      if (c[d] < lo[d]) lo[d] = c[d];
+      if (c[d] > hi[d]) hi[d] = c[d];
+    }
+  }
+  float size = hi[2] - lo[2];
+  if (hi[1] - lo[1] > size) size = hi[1] - lo[1];
+  if (hi[0] - lo[0] > size) size = hi[0] - lo[0];
+  const float fac = size > 0.f ? (float)(1.0 / size * (double)(1 << 18)) : 0.f;
+  if (box) { box[0] = lo[0]; box[1] = lo[1]; box[2] = lo[2]; box[3] = fac; }
+  for (int i = 0; i < n; i++) {
+    const float dx = (float)x[i] - lo[0], dy = (float)y[i] - lo[1], dz = (float)z[i] - lo[2];
+    const float sx = dx * fac, sy = dy * fac, sz = dz * fac;
+    keys[i] = orc_peano_hilbert_key((int)sx, (int)sy, (int)sz, 18);
+  }
+}
+
 typedef struct { uint64_t k; int i; } kv_t;
 static int cmp_kv(const void *a, const void *b) {
   const kv_t *x = (const kv_t *)a, *y = (const kv_t *)b;

@@ -60,3 +60,37 @@ def test_reference_driver_runs_on_this_library(tmp_path):
         assert abs(U - st["U"]) <= 1e-4 * abs(st["U"])
         assert abs(E - st["E"]) <= 1e-3 * abs(st["E"])
     sim.close()
+
+
+@pytest.mark.skipif(not os.path.exists(DRIVER), reason="reference driver not built (make -C oracle driver)")
+def test_reference_sort_order_equals_peano_key_mode(tmp_path):
+    """The driver Peano-Hilbert sorts every 100th iteration (step.cpp:26-31,
+    sort_bodies.cpp:119-186); a restart file at iteration 99 makes its first
+    step sort, so its restart.bin holds the particles in the reference's own
+    order.  That order must be the one the native context sorts into with
+    key_mode = Peano-Hilbert (distinct keys, so the reference's qsort has no
+    ties to order)."""
+    from cudasph_b200.simulation import Simulation, make_params
+    from oracle import oracle as O
+    n = 4096
+    ic = ics.polytrope(n, n_ngb=24, seed=23)
+    ic = {k: (v.astype(np.float32).astype(np.float64) if isinstance(v, np.ndarray) else v) for k, v in ic.items()}
+    k, _ = O.peano_keys(ic["x"], ic["y"], ic["z"])
+    assert np.unique(k).size == n
+    hdr = state_io.default_header(n, t_end=1e-12, dt_out=0.0, dt=0.0, global_time=0.0, iteration_number=99)
+    state_io.write_state(str(tmp_path / "init.bin"), hdr, ic)
+    r = subprocess.run([DRIVER, "init.bin"], cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "Peano-Hilbert sorting" in r.stderr
+    _, p = state_io.read_state(str(tmp_path / "restart.bin"))
+    sim = Simulation(ic, make_params(n_target=24.0, eos_mode=1, soft_mode=0, use_psi=1, key_mode=1))
+    sim.sort_bodies()
+    order = sim.order()
+    assert np.array_equal(order, O.sort_order(k))
+    sim.step()
+    sim.step()  # the driver's two steps; its restart.bin lists the particles in its sorted order
+    for c, tol in (("x", 1e-6), ("y", 1e-6), ("z", 1e-6), ("u", 1e-5)):
+        got = sim.get(c)[order]
+        assert np.max(np.abs(p[c] - got)) <= tol * np.max(np.abs(got)), c
+    sim.close()
+

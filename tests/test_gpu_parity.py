@@ -71,6 +71,63 @@ def test_morton_keys_and_sort_bitexact():
     assert np.array_equal(keys.cpu().numpy().view(np.uint64), k_ref[order])
 
 
+def test_peano_hilbert_keys_bitexact():
+    """The reference's Peano-Hilbert curve on the GPU: the reference's own
+    keys for 200 triplets (golden), the oracle's at every bit count 1..21
+    (including coordinate bits above the key's range, which are ignored), and
+    position keys with the reference's float quantisation."""
+    import os
+    import torch
+    from cudasph_b200._capi import SphError, check, lib
+    dev = torch.device("cuda:0")
+    s = torch.cuda.current_stream().cuda_stream
+
+    def gpu_keys(x, y, z, bits):
+        t = [torch.from_numpy(np.ascontiguousarray(a, np.int32)).to(dev) for a in (x, y, z)]
+        k = torch.empty(len(x), dtype=torch.int64, device=dev)
+        check(lib().cudasph_peano_hilbert_keys(len(x), t[0].data_ptr(), t[1].data_ptr(), t[2].data_ptr(), bits,
+                                               k.data_ptr(), s))
+        return k.cpu().numpy().view(np.uint64)
+
+    gold = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_tables.npz"))
+    ph_in = gold["ph_in"]
+    assert np.array_equal(gpu_keys(ph_in[:, 0], ph_in[:, 1], ph_in[:, 2], 18).view(np.int64), gold["ph_key"])
+    rs = np.random.default_rng(9)
+    for bits in range(1, 22):
+        c = rs.integers(0, 1 << 31, size=(4000, 3))
+        want = np.array([O.peano_hilbert_key(a, b, d, bits) for a, b, d in c], np.uint64)
+        assert np.array_equal(gpu_keys(c[:, 0], c[:, 1], c[:, 2], bits), want), bits
+    with pytest.raises(SphError):
+        check(lib().cudasph_peano_hilbert_keys(1, 0, 0, 0, 22, 0, s))
+    n = 200_003
+    x, y, z = (rs.normal(0, 1, n) for _ in range(3))
+    tx, ty, tz = (torch.from_numpy(a).to(dev) for a in (x, y, z))
+    keys = torch.empty(n, dtype=torch.int64, device=dev)
+    box = torch.empty(4, dtype=torch.float64, device=dev)
+    check(lib().cudasph_peano_keys(n, tx.data_ptr(), ty.data_ptr(), tz.data_ptr(), keys.data_ptr(), box.data_ptr(), s))
+    k_ref, box_ref = O.peano_keys(x, y, z)
+    assert np.array_equal(keys.cpu().numpy().view(np.uint64), k_ref)
+    assert np.array_equal(box.cpu().numpy(), box_ref)
+
+
+def test_peano_key_mode_sorts_in_the_reference_order(poly):
+    """key_mode = Peano-Hilbert: the context's sort is the stable order of
+    the reference's keys, and a step in that order gives the same physics as
+    one in Morton order (summation order only)."""
+    sim = _sim(poly, n_target=50.0, eos_mode=0, soft_mode=1, eps=0.01, key_mode=1)
+    sim.sort_bodies()
+    k, _ = O.peano_keys(poly["x"], poly["y"], poly["z"])
+    assert np.array_equal(sim.order(), O.sort_order(k))
+    ref = _sim(poly, n_target=50.0, eos_mode=0, soft_mode=1, eps=0.01)
+    sim.step(2)
+    ref.step(2)
+    assert np.array_equal(sim.n_ngb(), ref.n_ngb())
+    for f in ("x", "vx", "rho", "ax", "du", "gx", "phi"):
+        assert _rel(sim.get(f), ref.get(f)) < 1e-11, f
+    sim.close()
+    ref.close()
+
+
 def test_sort_permutes_state(poly):
     sim = _sim(poly, n_target=50.0, eos_mode=0, soft_mode=1, eps=0.01)
     sim.sort_bodies()

@@ -161,3 +161,39 @@ def test_pair_force_conserves_momentum(pipe):
     F = np.array([np.sum(s["m"] * h[k]) for k in ("ax", "ay", "az")])
     scale = np.sum(s["m"] * np.sqrt(h["ax"] ** 2 + h["ay"] ** 2 + h["az"] ** 2))
     assert np.max(np.abs(F)) < 1e-12 * scale
+
+
+def test_peano_hilbert_key_against_reference(tab):
+    """peano_hilbert_key (sort_bodies.cpp:66-105): the 200 keys the reference
+    made for random 18-bit triplets, bit for bit, and the curve's defining
+    properties at 3 bits: every cell gets a distinct key, and cells with
+    consecutive keys are face neighbours (a continuous curve)."""
+    got = np.array([O.peano_hilbert_key(a, b, c, 18) for a, b, c in tab["ph_in"]], np.int64)
+    assert np.array_equal(got, tab["ph_key"])
+    cells = {}
+    for x in range(8):
+        for y in range(8):
+            for z in range(8):
+                cells[O.peano_hilbert_key(x, y, z, 3)] = (x, y, z)
+    assert sorted(cells) == list(range(512))
+    for k in range(511):
+        assert sum(abs(a - b) for a, b in zip(cells[k], cells[k + 1])) == 1
+
+
+def test_peano_keys_of_positions_quantise_in_float():
+    """Positions are keyed as sort_bodies.cpp:121-160 does on its float4
+    state: float box, domain_fac = float(1.0 / size * 2^18), float offset and
+    scale, truncation, 18 bits (a coordinate at the far side wraps to its low
+    18 bits)."""
+    rs = np.random.default_rng(8)
+    x, y, z = (rs.normal(0, 1, 3000) for _ in range(3))
+    k, box = O.peano_keys(x, y, z)
+    f = [np.float32(a) for a in (x, y, z)]
+    lo = [a.min() for a in f]
+    size = max(f[2].max() - lo[2], max(f[1].max() - lo[1], f[0].max() - lo[0]))
+    fac = np.float32(1.0 / np.float64(size) * 262144.0)
+    assert np.array_equal(box, np.array([lo[0], lo[1], lo[2], fac], np.float64))
+    q = [((a - l) * fac).astype(np.int64) for a, l in zip(f, lo)]
+    want = np.array([O.peano_hilbert_key(a, b, c, 18) for a, b, c in zip(*q)], np.uint64)
+    assert np.array_equal(k, want)
+    assert max(int(a.max()) for a in q) == 262144  # the far side of the largest extent
