@@ -17,14 +17,15 @@
 // of its two children's threads to arrive combines them (parallel-axis shift
 // Q += M_k (3 s s - |s|^2 I), s = c_k - c; b = max(|s| + b_k)).
 //
-// Walk: one warp per SPH leaf (a "group" of 32 targets, whose float box the
-// SPH tree holds).  Each round pops up to sixteen internal nodes and tests
-// their two children, one per lane: a child node is accepted for the whole
-// group when b < theta * dmin, dmin = distance from c to the group's box (so
-// every particle of the node lies at least (1 - theta) dmin from every
-// target).  Accepted nodes go to a shared-memory list that all lanes sweep,
-// two nodes per packed f32x2 instruction, with the softened monopole +
-// quadrupole
+// Walk: one warp per SPH leaf of 32 targets, split into two groups where the
+// leaf straddles a boundary of the curve (see "sub-groups" below); each group
+// walks with the box of its own particles.  Each round pops up to sixteen
+// internal nodes and tests their two children, one per lane: a child node is
+// accepted for the whole group when b < theta * dmin, dmin = distance from c
+// to the group's box (so every particle of the node lies at least
+// (1 - theta) dmin from every target).  Accepted nodes go to a shared-memory
+// list that all lanes sweep, two nodes per packed f32x2 instruction, with the
+// softened monopole + quadrupole
 //   a = M r / s^3 - Q r / s^5 + (5/2) (r.Q.r) r / s^7,
 //   phi = -M / s - (1/2) (r.Q.r) / s^5,   r = c - x_i, s^2 = |r|^2 + eps^2;
 // child particles and opened nodes of at most kBucket particles go to a ring
@@ -51,12 +52,14 @@ static_assert(32 * kBucket + 32 <= kTgRing, "a round's particles fit the ring");
 // per internal node (n - 1 of them): moments cm = {cx, cy, cz, M},
 // q0 = {Qxx, Qyy, Qzz, Qxy}, q1 = {Qxz, Qyz, b, count}; children (an index
 // >= 0 is an internal node, ~p a particle); particle range; parent; arrival
-// counter of the bottom-up pass.  Per particle: its parent.
+// counter of the bottom-up pass.  Per particle: its parent.  One counter of
+// the groups the walk has handed out.
 struct TgWork {
   double4 *cm, *q0, *q1;
   int2 *child, *range;
   int *parent, *lparent;
   unsigned *flag;
+  unsigned *next_group;
 };
 
 static size_t al256(size_t b) { return (b + 255) / 256 * 256; }
@@ -64,7 +67,7 @@ static size_t al256(size_t b) { return (b + 255) / 256 * 256; }
 size_t tree_gravity_workspace_bytes(int n) {
   const size_t ni = n > 1 ? (size_t)n - 1 : 1;
   return 3 * al256(sizeof(double4) * ni) + 2 * al256(sizeof(int2) * ni) + al256(sizeof(int) * ni) +
-         al256(sizeof(int) * (size_t)(n > 0 ? n : 1)) + al256(sizeof(unsigned) * ni);
+         al256(sizeof(int) * (size_t)(n > 0 ? n : 1)) + al256(sizeof(unsigned) * ni) + 256;
 }
 
 static TgWork carve(void *ws, int n) {
@@ -78,7 +81,8 @@ static TgWork carve(void *ws, int n) {
   w.range = (int2 *)p; p += al256(sizeof(int2) * ni);
   w.parent = (int *)p; p += al256(sizeof(int) * ni);
   w.lparent = (int *)p; p += al256(sizeof(int) * (size_t)(n > 0 ? n : 1));
-  w.flag = (unsigned *)p;
+  w.flag = (unsigned *)p; p += al256(sizeof(unsigned) * ni);
+  w.next_group = (unsigned *)p;
   return w;
 }
 
@@ -192,9 +196,10 @@ __global__ void k_tree_moments(int n, const double4 *__restrict__ src, TgWork w)
 
 // -------------------------------- the walk -----------------------------------
 struct TreeGravArgs {
-  TreeView t;          // the SPH tree: the groups' boxes (level 0)
+  TreeView t;          // the SPH tree: its leaves are the groups
   TgWork w;            // the gravity tree
   const double4 *src;  // {x, y, z, m} per particle, tree order
+  const uint64_t *keys;  // the sorted keys of that order
   double4 *out;        // {gx, gy, gz, phi}
   unsigned *flags;
   float eps2, theta;
@@ -218,30 +223,103 @@ struct TgSmem {
   int stack[kTgStack];   // internal nodes to open
 };
 
-__global__ void __launch_bounds__(kTgWarps * 32) k_tree_gravity(TreeGravArgs a) {
-  __shared__ TgSmem smem[kTgWarps];
-  TgSmem &sm = smem[threadIdx.x >> 5];
-  const int grp = a.leaf0 + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  if (grp >= a.leaf1) return;
+// ---- sub-groups ----
+// A leaf of 32 consecutive particles can straddle a boundary of the curve and
+// then spans two distant clumps; its box, and with it the set of opened
+// nodes, is then far larger than either clump's (such a group sums most of a
+// star directly).  The leaf is therefore split where its keys split in the
+// radix tree (the first particle with the highest differing key bit set),
+// up to kTgSplitLevels times, wherever the larger half's extent is below
+// kTgSplitRatio of the whole part's: a compact group is not split, a
+// straddling one walks once per clump, with that clump's box and anchor.
+// Measured on the two-polytrope state (N = 262,144 and 1,048,576) and the
+// 4M cold sphere: ratio 0.35 with one level is fastest (1M, theta 0.5:
+// 12.0 ms unsplit, 5.6 ms); 0.5 or more levels also split compact leaves
+// (6.4 - 6.7 ms), 0.25 or less leaves the costliest straddlers whole (13 ms).
+constexpr int kTgSplitLevels = 1;
+constexpr double kTgSplitRatio = 0.35;
+
+__device__ __forceinline__ double warp_min(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// bounding box of the lanes in `mask` (lo, hi; every lane gets the result)
+__device__ __forceinline__ void lanes_box(bool in, double x, double y, double z, double *lo, double *hi) {
+  lo[0] = warp_min(in ? x : 1e300); hi[0] = warp_max(in ? x : -1e300);
+  lo[1] = warp_min(in ? y : 1e300); hi[1] = warp_max(in ? y : -1e300);
+  lo[2] = warp_min(in ? z : 1e300); hi[2] = warp_max(in ? z : -1e300);
+}
+
+__device__ __forceinline__ double box_extent(const double *lo, const double *hi) {
+  return fmax(fmax(hi[0] - lo[0], hi[1] - lo[1]), hi[2] - lo[2]);
+}
+
+// lanes [first, last] of the part that starts at lane `first` in the
+// part-start mask `starts` (last = the lane before the next start, or cnt - 1)
+__device__ __forceinline__ int part_last(unsigned starts, int first, int cnt) {
+  const unsigned above = first < 31 ? starts & (0xffffffffu << (first + 1)) : 0u;
+  return above ? __ffs(above) - 2 : cnt - 1;
+}
+
+__device__ __forceinline__ unsigned lane_range(int lo, int hi) {  // lanes lo..hi
+  const unsigned up = hi >= 31 ? 0xffffffffu : ((1u << (hi + 1)) - 1u);
+  return up & ~((1u << lo) - 1u);
+}
+
+// the walk of one group (SPH leaf `grp`) by the calling warp
+__device__ __forceinline__ void tree_group(const TreeGravArgs &a, TgSmem &sm, int grp) {
   const unsigned lane = lane_id();
   const int n = a.t.n;
   const int s = grp * kLeaf + (int)lane;
-  const bool valid = s < n;
-  const double4 anc = a.src[grp * kLeaf];
-  float xi = 0.f, yi = 0.f, zi = 0.f;
-  if (valid) {
-    const double4 p = a.src[s];
-    xi = (float)(p.x - anc.x); yi = (float)(p.y - anc.y); zi = (float)(p.z - anc.z);
+  const int cnt = min(kLeaf, n - grp * kLeaf);  // targets of this group (lanes 0 .. cnt-1)
+  const bool valid = (int)lane < cnt;
+  const double4 me = valid ? a.src[s] : a.src[grp * kLeaf];
+  const uint64_t key = valid ? a.keys[s] : 0ull;
+
+  // the group's parts (bit L of `starts` set: a part starts at lane L)
+  unsigned starts = 1u;
+  for (int lev = 0; lev < kTgSplitLevels; lev++) {
+    unsigned next = starts;
+    for (unsigned m = starts; m; m &= m - 1u) {
+      const int f = __ffs(m) - 1, l = part_last(starts, f, cnt);
+      if (l <= f) continue;
+      const uint64_t kf = __shfl_sync(0xffffffffu, key, f), kl = __shfl_sync(0xffffffffu, key, l);
+      if (kf == kl) continue;
+      const int top = 63 - __clzll((long long)(kf ^ kl));
+      const unsigned in = lane_range(f, l);
+      const unsigned upper = __ballot_sync(0xffffffffu, ((key >> top) & 1ull) != 0ull) & in;
+      const int sp = __ffs(upper) - 1;  // first lane of the upper half (kl has the bit: sp in (f, l])
+      const bool inp = (in >> lane) & 1u, ina = inp && (int)lane < sp, inb = inp && (int)lane >= sp;
+      double plo[3], phi[3], alo[3], ahi[3], blo[3], bhi[3];
+      lanes_box(inp, me.x, me.y, me.z, plo, phi);
+      lanes_box(ina, me.x, me.y, me.z, alo, ahi);
+      lanes_box(inb, me.x, me.y, me.z, blo, bhi);
+      if (fmax(box_extent(alo, ahi), box_extent(blo, bhi)) < kTgSplitRatio * box_extent(plo, phi))
+        next |= 1u << sp;
+    }
+    starts = next;
   }
-  const float4 gl = a.t.lo[a.t.base[0] + grp], gh = a.t.hi[a.t.base[0] + grp];
+
   const float eps2 = a.eps2;
   const double theta = a.theta;
   double ax = 0, ay = 0, az = 0, ap = 0;
   int nlist = 0;
   unsigned head = 0, tail = 0;  // ring positions (mod kTgRing)
   bool ok = true;
+  // per part: anchor, the lane's target relative to it, the part's box
+  double4 anc = me;
+  float xi = 0.f, yi = 0.f, zi = 0.f;
+  double glo[3] = {0, 0, 0}, ghi[3] = {0, 0, 0};
+  f32x2 X2 = 0ull, Y2 = 0ull, Z2 = 0ull;
 
-  const f32x2 X2 = pk2(xi, xi), Y2 = pk2(yi, yi), Z2 = pk2(zi, zi), E2 = pk2(eps2, eps2);
+  const f32x2 E2 = pk2(eps2, eps2);
   const f32x2 HALF5 = pk2(2.5f, 2.5f), MHALF = pk2(-0.5f, -0.5f), MONE = pk2(-1.f, -1.f);
   auto sweep_list = [&]() {
     __syncwarp();  // entries written by every lane are visible
@@ -320,99 +398,132 @@ __global__ void __launch_bounds__(kTgWarps * 32) k_tree_gravity(TreeGravArgs a) 
     __syncwarp();
   };
 
-  int sp = 0;
-  if (n < 2) {  // a single particle: no internal node
-    if (lane == 0) sm.ring[0] = 0;
-    tail = 1;
-  } else {
-    if (lane == 0) sm.stack[0] = 0;  // the root covers [0, n)
-    sp = 1;
-  }
-  __syncwarp();
-  while (sp > 0) {
-    // pop up to sixteen nodes; lane L tests child (L & 1) of popped node (L >> 1)
-    const int take = min(sp, 16);
-    const int slot = (int)(lane >> 1);
-    int node = -1;
-    if (slot < take) node = sm.stack[sp - 1 - slot];
-    sp -= take;
-    __syncwarp();
-    int ref = 0;
-    bool live = slot < take;
-    if (live) {
-      const int2 ch = a.w.child[node];
-      ref = (lane & 1u) ? ch.y : ch.x;
+  for (unsigned parts = starts; parts && ok; parts &= parts - 1u) {
+    const int f = __ffs(parts) - 1, l = part_last(starts, f, cnt);
+    const bool mine = (int)lane >= f && (int)lane <= l;
+    anc.x = __shfl_sync(0xffffffffu, me.x, f);
+    anc.y = __shfl_sync(0xffffffffu, me.y, f);
+    anc.z = __shfl_sync(0xffffffffu, me.z, f);
+    lanes_box(mine, me.x, me.y, me.z, glo, ghi);
+    xi = (float)(me.x - anc.x); yi = (float)(me.y - anc.y); zi = (float)(me.z - anc.z);
+    X2 = pk2(xi, xi); Y2 = pk2(yi, yi); Z2 = pk2(zi, zi);
+    const double sx = ax, sy = ay, sz = az, sph = ap;  // lanes of other parts keep these
+
+    int sp = 0;
+    if (n < 2) {  // a single particle: no internal node
+      if (lane == 0) sm.ring[0] = 0;
+      tail = 1;
+    } else {
+      if (lane == 0) sm.stack[0] = 0;  // the root covers [0, n)
+      sp = 1;
     }
-    bool accept = false, open = false;
-    int p0 = 0, pc = 0;  // source particles this lane hands to the ring
-    double4 c = make_double4(0, 0, 0, 0);
-    if (live && ref < 0) {
-      p0 = ~ref;
-      pc = 1;
-    } else if (live) {
-      c = a.w.cm[ref];
-      const double4 qb = a.w.q1[ref];
-      if (c.w > 0) {
-        const double ddx = fmax(fmax((double)gl.x - c.x, c.x - (double)gh.x), 0.0);
-        const double ddy = fmax(fmax((double)gl.y - c.y, c.y - (double)gh.y), 0.0);
-        const double ddz = fmax(fmax((double)gl.z - c.z, c.z - (double)gh.z), 0.0);
-        accept = qb.z < theta * sqrt(ddx * ddx + ddy * ddy + ddz * ddz);
-        if (!accept) {
-          if (qb.w <= (double)kBucket) {
-            p0 = a.w.range[ref].x;
-            pc = (int)qb.w;
-          } else {
-            open = true;
+    __syncwarp();
+    while (sp > 0) {
+      // pop up to sixteen nodes; lane L tests child (L & 1) of popped node (L >> 1)
+      const int take = min(sp, 16);
+      const int slot = (int)(lane >> 1);
+      int node = -1;
+      if (slot < take) node = sm.stack[sp - 1 - slot];
+      sp -= take;
+      __syncwarp();
+      int ref = 0;
+      bool live = slot < take;
+      if (live) {
+        const int2 ch = a.w.child[node];
+        ref = (lane & 1u) ? ch.y : ch.x;
+      }
+      bool accept = false, open = false;
+      int p0 = 0, pc = 0;  // source particles this lane hands to the ring
+      double4 c = make_double4(0, 0, 0, 0);
+      if (live && ref < 0) {
+        p0 = ~ref;
+        pc = 1;
+      } else if (live) {
+        c = a.w.cm[ref];
+        const double4 qb = a.w.q1[ref];
+        if (c.w > 0) {
+          const double ddx = fmax(fmax(glo[0] - c.x, c.x - ghi[0]), 0.0);
+          const double ddy = fmax(fmax(glo[1] - c.y, c.y - ghi[1]), 0.0);
+          const double ddz = fmax(fmax(glo[2] - c.z, c.z - ghi[2]), 0.0);
+          accept = qb.z < theta * sqrt(ddx * ddx + ddy * ddy + ddz * ddz);
+          if (!accept) {
+            if (qb.w <= (double)kBucket) {
+              p0 = a.w.range[ref].x;
+              pc = (int)qb.w;
+            } else {
+              open = true;
+            }
           }
         }
       }
-    }
-    // accepted nodes -> the list (swept first when it could overflow)
-    const unsigned am = __ballot_sync(0xffffffffu, accept);
-    if (am) {
-      if (nlist + __popc(am) > kTgList) sweep_list();
-      if (accept) {
-        const double4 qa = a.w.q0[ref], qb = a.w.q1[ref];
-        const int k = nlist + __popc(am & ((1u << lane) - 1u));
-        NodePair &e = sm.list[k >> 1];
-        const int h = k & 1;
-        e.x[h] = (float)(c.x - anc.x); e.y[h] = (float)(c.y - anc.y); e.z[h] = (float)(c.z - anc.z);
-        e.m[h] = (float)c.w;
-        e.qxx[h] = (float)qa.x; e.qyy[h] = (float)qa.y; e.qzz[h] = (float)qa.z; e.qxy[h] = (float)qa.w;
-        e.qxz[h] = (float)qb.x; e.qyz[h] = (float)qb.y;
+      // accepted nodes -> the list (swept first when it could overflow)
+      const unsigned am = __ballot_sync(0xffffffffu, accept);
+      if (am) {
+        if (nlist + __popc(am) > kTgList) sweep_list();
+        if (accept) {
+          const double4 qa = a.w.q0[ref], qb = a.w.q1[ref];
+          const int k = nlist + __popc(am & ((1u << lane) - 1u));
+          NodePair &e = sm.list[k >> 1];
+          const int h = k & 1;
+          e.x[h] = (float)(c.x - anc.x); e.y[h] = (float)(c.y - anc.y); e.z[h] = (float)(c.z - anc.z);
+          e.m[h] = (float)c.w;
+          e.qxx[h] = (float)qa.x; e.qyy[h] = (float)qa.y; e.qzz[h] = (float)qa.z; e.qxy[h] = (float)qa.w;
+          e.qxz[h] = (float)qb.x; e.qyz[h] = (float)qb.y;
+        }
+        nlist += __popc(am);
+        __syncwarp();
       }
-      nlist += __popc(am);
+      // particles -> the ring (warp prefix sum of the counts), then every full chunk is swept
+      int incl = pc;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if ((int)lane >= o) incl += v;
+      }
+      const int total = __shfl_sync(0xffffffffu, incl, 31);
+      if (total > 0) {
+        for (int k = 0; k < pc; k++) sm.ring[(tail + (unsigned)(incl - pc + k)) % kTgRing] = p0 + k;
+        tail += (unsigned)total;
+        while (tail - head >= 32u) sweep_chunk(32u);
+      }
+      // opened larger nodes -> the stack
+      const unsigned om = __ballot_sync(0xffffffffu, open);
+      const int nopen = __popc(om);
+      if (sp + nopen > kTgStack) {
+        ok = false;
+        break;
+      }
+      if (open) sm.stack[sp + nopen - 1 - __popc(om & ((1u << lane) - 1u))] = ref;
+      sp += nopen;
       __syncwarp();
     }
-    // particles -> the ring (warp prefix sum of the counts), then every full chunk is swept
-    int incl = pc;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int v = __shfl_up_sync(0xffffffffu, incl, o);
-      if ((int)lane >= o) incl += v;
-    }
-    const int total = __shfl_sync(0xffffffffu, incl, 31);
-    if (total > 0) {
-      for (int k = 0; k < pc; k++) sm.ring[(tail + (unsigned)(incl - pc + k)) % kTgRing] = p0 + k;
-      tail += (unsigned)total;
-      while (tail - head >= 32u) sweep_chunk(32u);
-    }
-    // opened larger nodes -> the stack
-    const unsigned om = __ballot_sync(0xffffffffu, open);
-    const int cnt = __popc(om);
-    if (sp + cnt > kTgStack) {
-      ok = false;
-      break;
-    }
-    if (open) sm.stack[sp + cnt - 1 - __popc(om & ((1u << lane) - 1u))] = ref;
-    sp += cnt;
     __syncwarp();
+    if (nlist > 0) sweep_list();
+    if (tail != head) sweep_chunk(tail - head);
+    if (!mine) {
+      ax = sx; ay = sy; az = sz; ap = sph;
+    }
   }
-  __syncwarp();
-  if (nlist > 0) sweep_list();
-  if (tail != head) sweep_chunk(tail - head);
   if (!ok && lane == 0) raise_flag(a.flags, SPH_FLAG_STACK_OVERFLOW);
   if (valid) a.out[s] = make_double4(a.G * ax, a.G * ay, a.G * az, a.G * ap);
+}
+
+// Persistent walk: one block per resident slot, and every warp takes the next
+// group from a counter until none is left.  Group costs differ several-fold
+// (a leaf in a sparse outer layer opens more nodes), and handing them out
+// one at a time lets a long group overlap the rest instead of ending the
+// launch alone on its SM.
+__global__ void __launch_bounds__(kTgWarps * 32, 5) k_tree_gravity(TreeGravArgs a) {
+  __shared__ TgSmem smem[kTgWarps];
+  TgSmem &sm = smem[threadIdx.x >> 5];
+  const unsigned groups = (unsigned)(a.leaf1 - a.leaf0);
+  for (;;) {
+    unsigned g = 0;
+    if (lane_id() == 0) g = atomicAdd(a.w.next_group, 1u);
+    g = __shfl_sync(0xffffffffu, g, 0);
+    if (g >= groups) break;
+    tree_group(a, sm, a.leaf0 + (int)g);
+  }
 }
 
 // keys: the sorted Morton keys of the current particle order (the sort's
@@ -435,11 +546,19 @@ int launch_tree_gravity(const TreeView &t, const uint64_t *keys, const double4 *
   shard_range(t.count[0], rank, world, l0, l1);
   if (l1 <= l0) return launches;
   TreeGravArgs a;
-  a.t = t; a.w = w; a.src = src; a.out = out; a.flags = flags;
+  a.t = t; a.w = w; a.src = src; a.keys = keys; a.out = out; a.flags = flags;
   a.eps2 = (float)(eps * eps); a.theta = (float)theta; a.G = G;
   a.leaf0 = (int)l0; a.leaf1 = (int)l1;
   const int warps = (int)(l1 - l0);
-  k_tree_gravity<<<(warps + kTgWarps - 1) / kTgWarps, kTgWarps * 32, 0, st>>>(a);
+  static int per_sm = 0;  // resident blocks per SM (the same on every device of one architecture)
+  if (per_sm == 0 && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tree_gravity, kTgWarps * 32, 0) != cudaSuccess)
+    per_sm = 1;
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    sms = 148;
+  const int blocks = min((warps + kTgWarps - 1) / kTgWarps, sms * max(per_sm, 1));
+  cudaMemsetAsync(w.next_group, 0, sizeof(unsigned), st);
+  k_tree_gravity<<<blocks, kTgWarps * 32, 0, st>>>(a);
   return launches + 1;
 }
 
