@@ -216,9 +216,16 @@ struct __align__(16) NodePair {
 };
 static_assert(sizeof(NodePair) == 80, "five 16-byte loads per pair");
 
+// A ring sweep's 32 staged source particles, in pairs laid out the same way
+// (particles 2j and 2j+1 as {p0, p1} per component).
+struct __align__(16) PartPair {
+  float x[2], y[2], z[2], m[2];
+};
+static_assert(sizeof(PartPair) == 32, "two 16-byte loads per pair");
+
 struct TgSmem {
   NodePair list[kTgList / 2];
-  float4 part[32];       // a sweep's staged source particles {x, y, z, m}
+  PartPair part[16];     // a sweep's staged source particles
   int ring[kTgRing];     // source particles awaiting their sweep
   int stack[kTgStack];   // internal nodes to open
 };
@@ -369,31 +376,43 @@ __device__ __forceinline__ void tree_group(const TreeGravArgs &a, TgSmem &sm, in
     nlist = 0;
     __syncwarp();  // every lane is done reading before the list is refilled
   };
-  // sweep 32 ring entries from `head` (fewer at the end: the rest padded far away and massless)
+  // sweep 32 ring entries from `head` (fewer at the end: the rest padded far
+  // away and massless), two sources per packed instruction
   auto sweep_chunk = [&](unsigned cnt) {
     __syncwarp();
-    float4 q = make_float4(1e18f, 1e18f, 1e18f, 0.f);
+    float qx = 1e18f, qy = 1e18f, qz = 1e18f, qm = 0.f;
     if (lane < cnt) {
       const double4 p = a.src[sm.ring[(head + lane) % kTgRing]];
-      q = make_float4((float)(p.x - anc.x), (float)(p.y - anc.y), (float)(p.z - anc.z), (float)p.w);
+      qx = (float)(p.x - anc.x); qy = (float)(p.y - anc.y); qz = (float)(p.z - anc.z); qm = (float)p.w;
     }
-    sm.part[lane] = q;
+    PartPair &d = sm.part[lane >> 1];
+    d.x[lane & 1] = qx; d.y[lane & 1] = qy; d.z[lane & 1] = qz; d.m[lane & 1] = qm;
     __syncwarp();
-    float px = 0.f, py = 0.f, pz = 0.f, pp = 0.f;
-#pragma unroll 8
-    for (int k = 0; k < 32; k++) {
-      const float4 p = sm.part[k];
-      const float dx = p.x - xi, dy = p.y - yi, dz = p.z - zi;
-      const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
-      const float inv = rsqrt_f32(r2);
-      const float sj = p.w * inv;
-      const float s3 = sj * inv * inv;
-      px = fmaf(dx, s3, px);
-      py = fmaf(dy, s3, py);
-      pz = fmaf(dz, s3, pz);
-      pp -= sj;
+    f32x2 px = 0ull, py = 0ull, pz = 0ull, pp = 0ull;
+#pragma unroll 4
+    for (int k = 0; k < 16; k++) {
+      const PartPair &e = sm.part[k];
+      const f32x2 ex = *reinterpret_cast<const f32x2 *>(e.x), ey = *reinterpret_cast<const f32x2 *>(e.y);
+      const f32x2 ez = *reinterpret_cast<const f32x2 *>(e.z), em = *reinterpret_cast<const f32x2 *>(e.m);
+      const f32x2 dx = sub2(ex, X2), dy = sub2(ey, Y2), dz = sub2(ez, Z2);
+      f32x2 r2 = fma2(dx, dx, E2);
+      r2 = fma2(dy, dy, r2);
+      r2 = fma2(dz, dz, r2);
+      float ra, rb;
+      upk2(r2, ra, rb);
+      const f32x2 inv = pk2(rsqrt_f32(ra), rsqrt_f32(rb));
+      const f32x2 sj = mul2(em, inv);
+      const f32x2 s3 = mul2(mul2(sj, inv), inv);
+      px = fma2(dx, s3, px);
+      py = fma2(dy, s3, py);
+      pz = fma2(dz, s3, pz);
+      pp = sub2(pp, sj);
     }
-    ax += px; ay += py; az += pz; ap += pp;
+    float a0, a1;
+    upk2(px, a0, a1); ax += (double)a0 + (double)a1;
+    upk2(py, a0, a1); ay += (double)a0 + (double)a1;
+    upk2(pz, a0, a1); az += (double)a0 + (double)a1;
+    upk2(pp, a0, a1); ap += (double)a0 + (double)a1;
     head += cnt;
     __syncwarp();
   };
