@@ -52,13 +52,25 @@ static_assert(32 * kBucket + 32 <= kTgRing, "a round's particles fit the ring");
 // per internal node (n - 1 of them): moments cm = {cx, cy, cz, M},
 // q0 = {Qxx, Qyy, Qzz, Qxy}, q1 = {Qxz, Qyz, b, count}; children (an index
 // >= 0 is an internal node, ~p a particle); particle range; parent; arrival
-// counter of the bottom-up pass.  Per particle: its parent.  One counter of
-// the groups the walk has handed out.
+// counter of the bottom-up pass.  Per particle: its parent.  Per child slot
+// of every internal node (2 (n - 1), indexed 2 node + side): what the walk
+// tests that child with, so one load answers it.  One counter of the groups
+// the walk has handed out.
+struct __align__(16) ChildRec {
+  float cx, cy, cz;  // centre of mass (float: the opening test only)
+  float b;           // radius, rounded up; -1 for a massless node
+  int ref;           // the child: an internal node, or ~particle
+  int first, count;  // its particles
+  int pad;
+};
+static_assert(sizeof(ChildRec) == 32, "one 32-byte record per child");
+
 struct TgWork {
   double4 *cm, *q0, *q1;
   int2 *child, *range;
   int *parent, *lparent;
   unsigned *flag;
+  ChildRec *rec;
   unsigned *next_group;
 };
 
@@ -67,7 +79,8 @@ static size_t al256(size_t b) { return (b + 255) / 256 * 256; }
 size_t tree_gravity_workspace_bytes(int n) {
   const size_t ni = n > 1 ? (size_t)n - 1 : 1;
   return 3 * al256(sizeof(double4) * ni) + 2 * al256(sizeof(int2) * ni) + al256(sizeof(int) * ni) +
-         al256(sizeof(int) * (size_t)(n > 0 ? n : 1)) + al256(sizeof(unsigned) * ni) + 256;
+         al256(sizeof(int) * (size_t)(n > 0 ? n : 1)) + al256(sizeof(unsigned) * ni) +
+         al256(sizeof(ChildRec) * 2 * ni) + 256;
 }
 
 static TgWork carve(void *ws, int n) {
@@ -82,6 +95,7 @@ static TgWork carve(void *ws, int n) {
   w.parent = (int *)p; p += al256(sizeof(int) * ni);
   w.lparent = (int *)p; p += al256(sizeof(int) * (size_t)(n > 0 ? n : 1));
   w.flag = (unsigned *)p; p += al256(sizeof(unsigned) * ni);
+  w.rec = (ChildRec *)p; p += al256(sizeof(ChildRec) * 2 * ni);
   w.next_group = (unsigned *)p;
   return w;
 }
@@ -122,6 +136,20 @@ __global__ void k_radix_tree(int n, const uint64_t *__restrict__ keys, TgWork w)
   const int right = (hi == gamma + 1) ? ~(gamma + 1) : gamma + 1;
   w.child[i] = make_int2(left, right);
   w.range[i] = make_int2(lo, hi);
+  // a particle child's record is complete here; an internal child's is
+  // finished by the moments pass
+  const int cref[2] = {left, right};
+#pragma unroll
+  for (int k = 0; k < 2; k++) {
+    ChildRec r;
+    r.cx = r.cy = r.cz = 0.f;
+    r.b = 0.f;
+    r.ref = cref[k];
+    r.first = cref[k] < 0 ? ~cref[k] : 0;
+    r.count = 1;
+    r.pad = 0;
+    w.rec[2 * i + k] = r;
+  }
   if (left < 0) w.lparent[gamma] = i;
   else w.parent[gamma] = i;
   if (right < 0) w.lparent[gamma + 1] = i;
@@ -190,7 +218,18 @@ __global__ void k_tree_moments(int n, const double4 *__restrict__ src, TgWork w)
     w.cm[node] = make_double4(cx, cy, cz, M);
     w.q0[node] = make_double4(Q[0], Q[1], Q[2], Q[3]);
     w.q1[node] = make_double4(Q[4], Q[5], b, (double)(r.y - r.x + 1));
-    node = w.parent[node];
+    const int up = w.parent[node];
+    if (up >= 0) {
+      ChildRec rec;
+      rec.cx = (float)cx; rec.cy = (float)cy; rec.cz = (float)cz;
+      rec.b = M > 0 ? __double2float_ru(b) : -1.f;
+      rec.ref = node;
+      rec.first = r.x;
+      rec.count = r.y - r.x + 1;
+      rec.pad = 0;
+      w.rec[2 * up + (w.child[up].x == node ? 0 : 1)] = rec;
+    }
+    node = up;
   }
 }
 
@@ -315,7 +354,7 @@ __device__ __forceinline__ void tree_group(const TreeGravArgs &a, TgSmem &sm, in
   }
 
   const float eps2 = a.eps2;
-  const double theta = a.theta;
+  const float theta = a.theta;
   double ax = 0, ay = 0, az = 0, ap = 0;
   int nlist = 0;
   unsigned head = 0, tail = 0;  // ring positions (mod kTgRing)
@@ -324,6 +363,7 @@ __device__ __forceinline__ void tree_group(const TreeGravArgs &a, TgSmem &sm, in
   double4 anc = me;
   float xi = 0.f, yi = 0.f, zi = 0.f;
   double glo[3] = {0, 0, 0}, ghi[3] = {0, 0, 0};
+  float flo[3] = {0.f, 0.f, 0.f}, fhi[3] = {0.f, 0.f, 0.f};  // the box rounded outward
   f32x2 X2 = 0ull, Y2 = 0ull, Z2 = 0ull;
 
   const f32x2 E2 = pk2(eps2, eps2);
@@ -340,6 +380,7 @@ __device__ __forceinline__ void tree_group(const TreeGravArgs &a, TgSmem &sm, in
     }
     f32x2 px = 0ull, py = 0ull, pz = 0ull, pp = 0ull;
     const int npair = (nlist + 1) >> 1;
+#pragma unroll 2
     for (int k = 0; k < npair; k++) {
       const NodePair &e = sm.list[k];
       const f32x2 ex = *reinterpret_cast<const f32x2 *>(e.x), ey = *reinterpret_cast<const f32x2 *>(e.y);
@@ -424,6 +465,11 @@ __device__ __forceinline__ void tree_group(const TreeGravArgs &a, TgSmem &sm, in
     anc.y = __shfl_sync(0xffffffffu, me.y, f);
     anc.z = __shfl_sync(0xffffffffu, me.z, f);
     lanes_box(mine, me.x, me.y, me.z, glo, ghi);
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      flo[d] = __double2float_rd(glo[d]);
+      fhi[d] = __double2float_ru(ghi[d]);
+    }
     xi = (float)(me.x - anc.x); yi = (float)(me.y - anc.y); zi = (float)(me.z - anc.z);
     X2 = pk2(xi, xi); Y2 = pk2(yi, yi); Z2 = pk2(zi, zi);
     const double sx = ax, sy = ay, sz = az, sph = ap;  // lanes of other parts keep these
@@ -445,33 +491,31 @@ __device__ __forceinline__ void tree_group(const TreeGravArgs &a, TgSmem &sm, in
       if (slot < take) node = sm.stack[sp - 1 - slot];
       sp -= take;
       __syncwarp();
-      int ref = 0;
-      bool live = slot < take;
-      if (live) {
-        const int2 ch = a.w.child[node];
-        ref = (lane & 1u) ? ch.y : ch.x;
+      const bool live = slot < take;
+      float4 r0 = make_float4(0.f, 0.f, 0.f, -1.f), r1 = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (live) {  // the child's record {cx, cy, cz, b}, {ref, first, count, -}
+        const float4 *rp = reinterpret_cast<const float4 *>(a.w.rec + 2 * node + (int)(lane & 1u));
+        r0 = __ldg(rp);
+        r1 = __ldg(rp + 1);
       }
+      const int ref = __float_as_int(r1.x);
       bool accept = false, open = false;
       int p0 = 0, pc = 0;  // source particles this lane hands to the ring
-      double4 c = make_double4(0, 0, 0, 0);
       if (live && ref < 0) {
         p0 = ~ref;
         pc = 1;
-      } else if (live) {
-        c = a.w.cm[ref];
-        const double4 qb = a.w.q1[ref];
-        if (c.w > 0) {
-          const double ddx = fmax(fmax(glo[0] - c.x, c.x - ghi[0]), 0.0);
-          const double ddy = fmax(fmax(glo[1] - c.y, c.y - ghi[1]), 0.0);
-          const double ddz = fmax(fmax(glo[2] - c.z, c.z - ghi[2]), 0.0);
-          accept = qb.z < theta * sqrt(ddx * ddx + ddy * ddy + ddz * ddz);
-          if (!accept) {
-            if (qb.w <= (double)kBucket) {
-              p0 = a.w.range[ref].x;
-              pc = (int)qb.w;
-            } else {
-              open = true;
-            }
+      } else if (live && r0.w >= 0.f) {
+        const float ddx = fmaxf(fmaxf(flo[0] - r0.x, r0.x - fhi[0]), 0.f);
+        const float ddy = fmaxf(fmaxf(flo[1] - r0.y, r0.y - fhi[1]), 0.f);
+        const float ddz = fmaxf(fmaxf(flo[2] - r0.z, r0.z - fhi[2]), 0.f);
+        accept = r0.w < theta * sqrtf(ddx * ddx + ddy * ddy + ddz * ddz);
+        if (!accept) {
+          const int count = __float_as_int(r1.z);
+          if (count <= kBucket) {
+            p0 = __float_as_int(r1.y);
+            pc = count;
+          } else {
+            open = true;
           }
         }
       }
@@ -480,7 +524,7 @@ __device__ __forceinline__ void tree_group(const TreeGravArgs &a, TgSmem &sm, in
       if (am) {
         if (nlist + __popc(am) > kTgList) sweep_list();
         if (accept) {
-          const double4 qa = a.w.q0[ref], qb = a.w.q1[ref];
+          const double4 c = a.w.cm[ref], qa = a.w.q0[ref], qb = a.w.q1[ref];
           const int k = nlist + __popc(am & ((1u << lane) - 1u));
           NodePair &e = sm.list[k >> 1];
           const int h = k & 1;
