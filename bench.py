@@ -307,12 +307,14 @@ def adjoint_cost(steps=5, warmup=3, headline_n=None):
     return out
 
 
-def tree_gravity(ic, thetas=(0.3, 0.5), reps=3, params=None):
+def tree_gravity(ic, thetas=(0.3, 0.5), reps=3, params=None, step_reps=3):
     """The opt-in Barnes-Hut gravity (grav_mode = tree, quadrupoles) on the
-    same state as the headline: CUDA-event time of the gravity phase (node
-    moments + walk) per opening angle and its RMS force error against the
-    direct mixed-precision sum (itself within 4e-8 of FP64 on this workload).
-    The direct sum stays the headline path."""
+    same state as the headline: CUDA-event time of the gravity phase (radix
+    tree + node moments + walk) per opening angle and its RMS force error
+    against the direct mixed-precision sum (itself within 4e-8 of FP64 on
+    this workload); then `step_reps` whole steps in that mode after one
+    warm-up step (CUDA-event span on the context's stream), the throughput a
+    run with tree gravity gets.  The direct sum stays the headline path."""
     from cudasph_b200.simulation import Simulation, make_params
     params = params or WORKLOAD_PARAMS
     d = Simulation(ic, make_params(**dict(params, precision=1)))
@@ -333,6 +335,12 @@ def tree_gravity(ic, thetas=(0.3, 0.5), reps=3, params=None):
         g = np.stack([s.get(k) for k in ("gx", "gy", "gz")], 1)
         out[f"theta_{th}"] = {"ms": ph["gravity"][0] / reps, "rms_force_rel_vs_direct": rms_rel(g, gd),
                               "flags": s.device_status()}
+        if step_reps > 0:
+            s.step(1)
+            s.synchronize()
+            step_ms = step_span_ms(s, step_reps) / step_reps
+            out[f"theta_{th}"].update(step_ms=step_ms, particle_steps_per_s=ic["x"].size / (step_ms * 1e-3),
+                                      step_flags=s.device_status())
         s.close()
     return out
 
