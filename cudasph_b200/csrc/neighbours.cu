@@ -31,6 +31,7 @@ struct WarpSmem {
   int stack[kStack];
   double sx[kLeaf], sy[kLeaf], sz[kLeaf];
   float4 sf[kLeaf];  // anchor-relative FP32 copies for the pre-filter
+  double tx[kLeaf], ty[kLeaf], tz[kLeaf];  // the warp's own particles (the targets)
 };
 
 // Conservative FP32 pre-filter of the neighbour predicate.  Coordinates are
@@ -257,6 +258,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 6) k_solve_range(SolveArg
     xi = p.x; yi = p.y; zi = p.z; w = p.w;
   }
   const Prefilter pf = make_prefilter(valid && w > 0, xi, yi, zi);
+  sm.tx[lane_id()] = xi;
+  sm.ty[lane_id()] = yi;
+  sm.tz[lane_id()] = zi;
+  __syncwarp();
+  const size_t colbase = (size_t)leaf * a.cap * kLeaf;  // the warp's block of list / dcache
   int phase = (valid && w > 0) ? kBr0 : kDone;
   double dx = 0, f = 0, x_left = 0, f_try = 0, rx = 0, ry = 0;
   int iter = 0, keep = 0, nev = 0;
@@ -290,9 +296,45 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 6) k_solve_range(SolveArg
       int c = 0;
       const LaneBox lb = lane_query_box(xi, yi, zi, r);
       const unsigned onmask = share_lane_boxes(sm, lb, on);
+      const bool any_dwalk = __any_sync(kFull, dwalk);
       stack_ok &= walk_leaves(a.t, ql, qh, sm.lbox, onmask, sm.stack, [&](int lj, const float *bl, const float *bh) {
-        stage_leaf(a.pos, n, lj, sm, pf);
         const int cntj = min(kLeaf, n - lj * kLeaf);
+        if (!any_dwalk) {
+          // Cache fills only: transposed.  Lane k holds candidate k of the
+          // leaf; for every lane t whose box meets the leaf, all 32 lanes
+          // apply t's exact predicate at once and a ballot appends the hits
+          // to t's column in ascending k -- the same entries, order and
+          // FP64 d2 as t testing the leaf itself, in |targets| rounds
+          // instead of 32 (a lane needs about half the leaves its warp
+          // visits).
+          const unsigned tm = __ballot_sync(kFull, on && lane_box_hits(lb, bl, bh));
+          if (!tm) return;
+          double xk = 1e300, yk = 1e300, zk = 1e300;  // past the last particle: never a neighbour
+          if ((int)lane_id() < cntj) {
+            const double4 p = ld4(a.pos + lj * kLeaf + (int)lane_id());
+            xk = p.x; yk = p.y; zk = p.z;
+          }
+          const int jk = lj * kLeaf + (int)lane_id();
+          for (unsigned m = tm; m; m &= m - 1u) {
+            const int t = __ffs(m) - 1;
+            const double r2t = __shfl_sync(kFull, r2, t);
+            const double d2 = ds2_exact(sm.tx[t] - xk, sm.ty[t] - yk, sm.tz[t] - zk);
+            const bool hit = d2 < r2t;
+            const unsigned hm = __ballot_sync(kFull, hit);
+            const int base = __shfl_sync(kFull, c, t);
+            if (hit) {
+              const int idx = base + __popc(hm & ((1u << lane_id()) - 1u));
+              if (idx < cap) {
+                const size_t off = colbase + (size_t)idx * kLeaf + (size_t)t;
+                a.list[off] = jk;
+                a.dcache[off] = d2;
+              }
+            }
+            if ((int)lane_id() == t) c += __popc(hm);
+          }
+          return;
+        }
+        stage_leaf(a.pos, n, lj, sm, pf);
         if (on && lane_box_hits(lb, bl, bh)) {
 #pragma unroll 8
           for (int k = 0; k < cntj; k++) {
