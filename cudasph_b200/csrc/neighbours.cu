@@ -315,22 +315,38 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 6) k_solve_range(SolveArg
             xk = p.x; yk = p.y; zk = p.z;
           }
           const int jk = lj * kLeaf + (int)lane_id();
-          for (unsigned m = tm; m; m &= m - 1u) {
-            const int t = __ffs(m) - 1;
-            const double r2t = __shfl_sync(kFull, r2, t);
-            const double d2 = ds2_exact(sm.tx[t] - xk, sm.ty[t] - yk, sm.tz[t] - zk);
-            const bool hit = d2 < r2t;
-            const unsigned hm = __ballot_sync(kFull, hit);
-            const int base = __shfl_sync(kFull, c, t);
-            if (hit) {
-              const int idx = base + __popc(hm & ((1u << lane_id()) - 1u));
+          const unsigned below = (1u << lane_id()) - 1u;
+          unsigned m = tm;
+          while (m) {  // two targets per round: independent chains overlap
+            const int t0 = __ffs(m) - 1;
+            m &= m - 1u;
+            const int t1 = m ? __ffs(m) - 1 : t0;
+            const bool two = m != 0u;
+            m &= m - 1u;
+            const double r20 = __shfl_sync(kFull, r2, t0), r21 = __shfl_sync(kFull, r2, t1);
+            const double d20 = ds2_exact(sm.tx[t0] - xk, sm.ty[t0] - yk, sm.tz[t0] - zk);
+            const double d21 = ds2_exact(sm.tx[t1] - xk, sm.ty[t1] - yk, sm.tz[t1] - zk);
+            const bool h0 = d20 < r20, h1 = two && d21 < r21;
+            const unsigned hm0 = __ballot_sync(kFull, h0), hm1 = __ballot_sync(kFull, h1);
+            const int b0 = __shfl_sync(kFull, c, t0), b1 = __shfl_sync(kFull, c, t1);
+            if (h0) {
+              const int idx = b0 + __popc(hm0 & below);
               if (idx < cap) {
-                const size_t off = colbase + (size_t)idx * kLeaf + (size_t)t;
+                const size_t off = colbase + (size_t)idx * kLeaf + (size_t)t0;
                 a.list[off] = jk;
-                a.dcache[off] = d2;
+                a.dcache[off] = d20;
               }
             }
-            if ((int)lane_id() == t) c += __popc(hm);
+            if (h1) {
+              const int idx = b1 + __popc(hm1 & below);
+              if (idx < cap) {
+                const size_t off = colbase + (size_t)idx * kLeaf + (size_t)t1;
+                a.list[off] = jk;
+                a.dcache[off] = d21;
+              }
+            }
+            if ((int)lane_id() == t0) c += __popc(hm0);
+            if ((int)lane_id() == t1) c += __popc(hm1);  // t1 != t0 whenever hm1 != 0
           }
           return;
         }
