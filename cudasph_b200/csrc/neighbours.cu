@@ -225,6 +225,8 @@ enum { kBr0 = 0, kBr1 = 1, kSolve = 2, kDone = 3 };
 // radius of a candidate cache relative to the range that fills it: one
 // clamped Newton step of the bracket (f_scale = 10 %) stays inside it
 constexpr double kCacheMargin = 1.15;
+constexpr int kEvalBatch = 4;     // cache entries loaded ahead per evaluation step
+constexpr int kCompactBatch = 8;  // cache entries loaded ahead per compaction step
 
 // dev_solve_range (dev_solve_range.cu:137-189): per particle, bracket the
 // root of f(w) = sum_j ig(2 r_ij / w) - N_target with clamped Newton steps
@@ -387,12 +389,19 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 6) k_solve_range(SolveArg
       }
     }
     if (iterate && !direct && w2 <= cache_r2) {
-      for (int k = 0; k < ncache; k++) {
-        const double d2 = dc[(size_t)k * kLeaf];
-        if (d2 < w2) {
-          const double u = 2 * sqrt(d2) / w;
-          sf += k_ig<double>(u);
-          sg -= k_digdh<double>(u);
+      // the cache does not fit in L2 at large N: load a batch of entries
+      // before using any (the sums keep the entries' order)
+      for (int k0 = 0; k0 < ncache; k0 += kEvalBatch) {
+        double d2[kEvalBatch];
+#pragma unroll
+        for (int q = 0; q < kEvalBatch; q++) d2[q] = k0 + q < ncache ? dc[(size_t)(k0 + q) * kLeaf] : w2;
+#pragma unroll
+        for (int q = 0; q < kEvalBatch; q++) {
+          if (d2[q] < w2) {
+            const double u = 2 * sqrt(d2[q]) / w;
+            sf += k_ig<double>(u);
+            sg -= k_digdh<double>(u);
+          }
         }
       }
       evaluated = true;
@@ -475,10 +484,23 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 6) k_solve_range(SolveArg
     // the final list: the cached entries inside the final range, in order
     const double w2 = __dmul_rn(w, w);
     int c = 0;
-    for (int k = 0; k < ncache; k++) {
-      if (dc[(size_t)k * kLeaf] < w2) {
-        lst[(size_t)c * kLeaf] = lst[(size_t)k * kLeaf];
-        c++;
+    // batches loaded before any store: a store goes to a slot c <= k below
+    // every slot a later batch reads
+    for (int k0 = 0; k0 < ncache; k0 += kCompactBatch) {
+      double d2[kCompactBatch];
+      int j[kCompactBatch];
+#pragma unroll
+      for (int q = 0; q < kCompactBatch; q++) {
+        const bool in = k0 + q < ncache;
+        d2[q] = in ? dc[(size_t)(k0 + q) * kLeaf] : w2;
+        j[q] = in ? lst[(size_t)(k0 + q) * kLeaf] : 0;
+      }
+#pragma unroll
+      for (int q = 0; q < kCompactBatch; q++) {
+        if (d2[q] < w2) {
+          lst[(size_t)c * kLeaf] = j[q];
+          c++;
+        }
       }
     }
     cnt_list = c;
