@@ -42,10 +42,23 @@ __global__ void __launch_bounds__(128) k_density(HydroArgs a) {
   const int *lst = a.list + (size_t)leaf * a.cap * kLeaf + lane;
   const double w = pi.w;
   double dens = 0, om = 0, ps = 0, sdig = 0, div = 0, cx = 0, cy = 0, cz = 0;
+  // the neighbours' records are gathered one pair ahead of their use and
+  // the list entries two ahead, so the loads overlap the pair arithmetic
+  int jn = cnt > 1 ? __ldg(lst + kLeaf) : 0;
+  double4 pn = make_double4(0, 0, 0, 0), vn = pn;
+  if (cnt > 0) {
+    const int j0 = __ldg(lst);
+    pn = ld4(a.pos + j0);
+    vn = ld4(a.vel + j0);
+  }
   for (int k = 0; k < kmax; k++) {
     if (k < cnt) {
-      const int j = __ldg(lst + (size_t)k * kLeaf);
-      const double4 pj = ld4(a.pos + j), vj = ld4(a.vel + j);
+      const double4 pj = pn, vj = vn;
+      if (k + 1 < cnt) {
+        pn = ld4(a.pos + jn);
+        vn = ld4(a.vel + jn);
+        if (k + 2 < cnt) jn = __ldg(lst + (size_t)(k + 2) * kLeaf);
+      }
       const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
       const double u = 2 * sqrt(ds2_exact(dx, dy, dz)) / w;
       const double mj = vj.w;
