@@ -94,6 +94,7 @@ struct sph_ctx {
   uint32_t *vals = nullptr;
   void *sort_scratch = nullptr;
   double *bbox_part = nullptr, *box4 = nullptr;
+  double4 *aux = nullptr;  // per-particle factors of the hydro pair loop (scratch)
   double4 *gsrc = nullptr;
   double *gh2 = nullptr;
   int *mass_mixed = nullptr;  // 0 when all masses are equal (set with the gravity sources)
@@ -246,7 +247,7 @@ HydroArgs hydro_args(sph_ctx *c) {
   a.nleaf = c->tree.count[0];
   a.cap = c->list_cap;
   a.pos = F.pos; a.vel = F.vel; a.hyd = F.hyd; a.dd = F.dd; a.dots = F.dots; a.vsig = F.vsig;
-  a.n_ngb = c->n_ngb; a.list = c->list; a.ngb_acc = nullptr;
+  a.n_ngb = c->n_ngb; a.list = c->list; a.ngb_acc = nullptr; a.aux = c->aux;
   a.alpha = c->p.av_alpha; a.beta = c->p.av_beta; a.gamma = c->p.gamma;
   a.use_psi = use_psi(c->p);
   a.jside = 1;
@@ -294,7 +295,7 @@ extern "C" int cudasph_destroy(sph_ctx *c) {
   }
   cudaFree(c->old); cudaFree(c->n_ngb); cudaFree(c->nevals); cudaFree(c->list); cudaFree(c->dcache);
   cudaFree(c->tlo); cudaFree(c->thi); cudaFree(c->tgws); cudaFree(c->keys); cudaFree(c->vals); cudaFree(c->sort_scratch);
-  cudaFree(c->bbox_part); cudaFree(c->box4); cudaFree(c->gsrc); cudaFree(c->gh2); cudaFree(c->mass_mixed); cudaFree(c->xbuf); cudaFree(c->flags);
+  cudaFree(c->bbox_part); cudaFree(c->box4); cudaFree(c->aux); cudaFree(c->gsrc); cudaFree(c->gh2); cudaFree(c->mass_mixed); cudaFree(c->xbuf); cudaFree(c->flags);
   cudaFree(c->sc); cudaFree(c->fin_part); cudaFree(c->flat); cudaFree(c->slot_of);
   cudaFree(c->pre_acc); cudaFree(c->xb); cudaFree(c->vb); cudaFree(c->ab); cudaFree(c->vpb); cudaFree(c->vpup);
   cudaFree(c->rhob); cudaFree(c->Pb); cudaFree(c->omb); cudaFree(c->psib); cudaFree(c->divb); cudaFree(c->curlb);
@@ -354,6 +355,7 @@ extern "C" int cudasph_create(const sph_params *params, int n, int device, sph_c
   TRY_ALLOC(dalloc((char **)&c->sort_scratch, radix_scratch_bytes(n)));
   TRY_ALLOC(dalloc(&c->bbox_part, 148 * 2 * 6));
   TRY_ALLOC(dalloc(&c->box4, 4));
+  TRY_ALLOC(dalloc(&c->aux, n));
   TRY_ALLOC(dalloc(&c->gsrc, n));
   TRY_ALLOC(dalloc(&c->gh2, n));
   TRY_ALLOC(dalloc(&c->mass_mixed, 1));

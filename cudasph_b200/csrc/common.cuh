@@ -53,6 +53,7 @@ struct HydroArgs {
   double *vsig;
   const int *n_ngb, *list;
   double *ngb_acc;  // optional, list layout: m_i * acc per pair
+  double4 *aux;     // per particle {c, P / rho^2, Balsara factor, 0}, written by launch_hydro
   double alpha, beta, gamma;
   int use_psi;
   int jside;  // 1: add the j-side pair force with atomics; 0: leave it to the caller

@@ -161,21 +161,32 @@ __global__ void k_pressure(int n, double4 *__restrict__ hyd, int eos_mode, doubl
   hyd[i].y = P;
 }
 
-// dev_art_visc.cu:8-32 in FP64
-__device__ __forceinline__ void art_visc(double range_i, double range_j, double ds, double drdv, double rho_i,
-                                         double P_i, double div_i, double curl_i, double rho_j, double P_j,
-                                         double div_j, double curl_j, double alpha, double beta, double gamma,
-                                         double &visc, double &vsig) {
-  double ci = sqrt(gamma * P_i / rho_i);
-  double cj = sqrt(gamma * P_j / rho_j);
-  double av = 0, vs = ci + cj;
+// The factors of dev_art_visc.cu:8-32 that depend on one particle only --
+// sound speed c = sqrt(gamma P / rho), P / rho^2 and the Balsara factor
+// |div| / (|div| + |curl| + 1e-4 c / h) -- computed once per particle with
+// the same operations the pair formula applies to them, so the pair loop
+// gathers one record {c, P / rho^2, B, 0} per neighbour instead of hyd and
+// dd and computes neither square root nor those divisions per pair.
+__global__ void k_hydro_prep(int n, const double4 *__restrict__ pos, const double4 *__restrict__ hyd,
+                             const double4 *__restrict__ dd, double gamma, double4 *__restrict__ aux) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double range = pos[i].w;
+  const double4 h = hyd[i], d = dd[i];
+  const double c = sqrt(gamma * h.y / h.x);
+  const double b = fabs(d.x) / (fabs(d.x) + d.y + 0.0001 * c / (0.5 * range));
+  aux[i] = make_double4(c, h.y / (h.x * h.x), b, 0.0);
+}
+
+// dev_art_visc.cu:8-32 on the per-particle factors of k_hydro_prep
+__device__ __forceinline__ void art_visc_pre(double ds, double drdv, const double4 &fi, const double4 &fj,
+                                             double alpha, double beta, double &visc, double &vsig) {
+  double av = 0, vs = fi.x + fj.x;
   if (drdv < 0) {
     vs -= beta * drdv / ds;
-    av = drdv / ((ci + cj) * ds);
-    const double bi = fabs(div_i) / (fabs(div_i) + curl_i + 0.0001 * ci / (0.5 * range_i));
-    const double bj = fabs(div_j) / (fabs(div_j) + curl_j + 0.0001 * cj / (0.5 * range_j));
-    av *= (bi + bj);
-    av = (P_i / (rho_i * rho_i) + P_j / (rho_j * rho_j)) * (-alpha * av + beta * av * av);
+    av = drdv / ((fi.x + fj.x) * ds);
+    av *= (fi.z + fj.z);
+    av = (fi.y + fj.y) * (-alpha * av + beta * av * av);
   }
   visc = av;
   vsig = vs;
@@ -191,13 +202,14 @@ __global__ void __launch_bounds__(128, 6) k_hydro(HydroArgs a) {
   const int s = leaf * kLeaf + lane;
   const bool valid = s < a.n;
   double4 pi = make_double4(0, 0, 0, 0), vi = make_double4(0, 0, 0, 1), hi4 = make_double4(0, 0, 0, 0),
-          di = make_double4(0, 0, 0, 0);
+          di = make_double4(0, 0, 0, 0), fi = make_double4(0, 0, 0, 0);
   int cnt = 0;
   if (valid) {
     pi = a.pos[s];
     vi = a.vel[s];
     hi4 = a.hyd[s];
     di = a.dd[s];
+    fi = a.aux[s];
     cnt = min(a.n_ngb[s], a.cap);
   }
   const int kmax = leaf_max_count(cnt);
@@ -210,15 +222,14 @@ __global__ void __launch_bounds__(128, 6) k_hydro(HydroArgs a) {
   for (int k = 0; k < kmax; k++) {
     if (k < cnt) {
       const int j = __ldg(lst + (size_t)k * kLeaf);
-      const double4 pj = ld4(a.pos + j), vj = ld4(a.vel + j), hj = ld4(a.hyd + j), dj = ld4(a.dd + j);
+      const double4 pj = ld4(a.pos + j), vj = ld4(a.vel + j), fj = ld4(a.aux + j);
       const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
       const double dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
       const double ds = sqrt(ds2_exact(dx, dy, dz));
       const double u = ds / hh;
       const double drdv = dx * dvx + dy * dvy + dz * dvz;
       double visc, vs;
-      art_visc(pi.w, pj.w, ds, drdv, hi4.x, hi4.y, di.x, di.y, hj.x, hj.y, dj.x, dj.y, a.alpha, a.beta, a.gamma,
-               visc, vs);
+      art_visc_pre(ds, drdv, fi, fj, a.alpha, a.beta, visc, vs);
       if (vs > vmax) vmax = vs;
       const double dwu = k_dw<double>(u), digu = k_dig<double>(u);
       const double mj = vj.w;
@@ -258,8 +269,10 @@ int launch_pressure(int n, double4 *hyd, int eos_mode, double gamma, unsigned *f
 }
 int launch_hydro(const HydroArgs &a, cudaStream_t st) {
   if (a.leaf1 <= a.leaf0) return 0;
+  // every particle's factors: a shard's pairs reach outside its own leaves
+  k_hydro_prep<<<(a.n + 255) / 256, 256, 0, st>>>(a.n, a.pos, a.hyd, a.dd, a.gamma, a.aux);
   k_hydro<<<((a.leaf1 - a.leaf0) * 32 + 127) / 128, 128, 0, st>>>(a);
-  return 1;
+  return 2;
 }
 
 }  // namespace sph
