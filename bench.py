@@ -219,7 +219,9 @@ SPH_BYTES = {
 
 # bytes of neighbour records each pair gathers (served by L1/L2): density
 # reads pos + vel of j, hydro pos + vel + hyd + dd of j
-SPH_GATHER = {"density": 64, "hydro": 128}
+# bytes gathered per pair: the neighbour's pos + vel (density); pos + vel +
+# its per-particle factors {c, P / rho^2, Balsara} (hydro)
+SPH_GATHER = {"density": 64, "hydro": 96}
 
 
 def sph_bandwidth(ph, steps, n, nbar):
