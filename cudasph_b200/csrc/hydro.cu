@@ -183,8 +183,9 @@ __device__ __forceinline__ void art_visc_pre(double ds, double drdv, const doubl
                                              double alpha, double beta, double &visc, double &vsig) {
   double av = 0, vs = fi.x + fj.x;
   if (drdv < 0) {
-    vs -= beta * drdv / ds;
-    av = drdv / ((fi.x + fj.x) * ds);
+    const double mu = drdv / ds;  // the approach speed along the pair
+    vs -= beta * mu;
+    av = mu / (fi.x + fj.x);
     av *= (fi.z + fj.z);
     av = (fi.y + fj.y) * (-alpha * av + beta * av * av);
   }
@@ -218,6 +219,11 @@ __global__ void __launch_bounds__(128, 6) k_hydro(HydroArgs a) {
   const double prho2 = (hi4.x > 0) ? hi4.y / (hi4.x * hi4.x) : 0;
   const double h2 = hh * hh, h5 = h2 * h2 * hh;
   const double psi_i = a.use_psi ? di.w : 0;
+  // per-particle reciprocals and factors: the pair loop divides only by the
+  // neighbour's mass (and, in compression, by ds and c_i + c_j)
+  const double ihh = 1.0 / hh, ih5 = 1.0 / h5;
+  const double gi = (prho2 * di.z + 0.5 * psi_i) / h2;  // grad-h term of the force
+  const double ei = prho2 * di.z / h2;                   // grad-h term of du/dt
   double axi = 0, ayi = 0, azi = 0, udot = 0, vmax = 0;
   for (int k = 0; k < kmax; k++) {
     if (k < cnt) {
@@ -226,15 +232,15 @@ __global__ void __launch_bounds__(128, 6) k_hydro(HydroArgs a) {
       const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
       const double dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
       const double ds = sqrt(ds2_exact(dx, dy, dz));
-      const double u = ds / hh;
+      const double u = ds * ihh;
       const double drdv = dx * dvx + dy * dvy + dz * dvz;
       double visc, vs;
       art_visc_pre(ds, drdv, fi, fj, a.alpha, a.beta, visc, vs);
       if (vs > vmax) vmax = vs;
       const double dwu = k_dw<double>(u), digu = k_dig<double>(u);
       const double mj = vj.w;
-      double acc = (prho2 + 0.5 * visc) * dwu / h5;
-      acc -= (prho2 * di.z + 0.5 * psi_i) / mj * digu / h2;
+      const double ta = (prho2 + 0.5 * visc) * dwu * ih5;
+      const double acc = ta - gi * digu / mj;
       axi -= mj * acc * dx;
       ayi -= mj * acc * dy;
       azi -= mj * acc * dz;
@@ -245,8 +251,7 @@ __global__ void __launch_bounds__(128, 6) k_hydro(HydroArgs a) {
         atomicAdd(&a.dots[j].y, nacc * dy);
         atomicAdd(&a.dots[j].z, nacc * dz);
       }
-      double ud = mj * (prho2 + 0.5 * visc) * dwu / h5;
-      ud -= prho2 * di.z * digu / h2;
+      const double ud = mj * ta - ei * digu;
       udot += ud * drdv;
     }
   }
