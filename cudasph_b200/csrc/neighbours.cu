@@ -113,6 +113,31 @@ __device__ __forceinline__ LaneBox lane_query_box(double x, double y, double z, 
   return b;
 }
 
+// This lane's query ball for the box test below: centre rounded to float
+// and the squared radius widened to cover every rounding of the float test
+// (the centre's rounding, the subtractions, squares and sums: under
+// 4e-7 (|x| + |y| + |z|) absolute and 1e-6 relative), so a leaf that holds a
+// j with |x_j - x| < r always passes.
+struct LaneBall {
+  float x, y, z, r2;
+};
+
+__device__ __forceinline__ LaneBall lane_ball(double x, double y, double z, double r) {
+  const double rr = r * (1.0 + 1e-6) + 4e-7 * (fabs(x) + fabs(y) + fabs(z));
+  LaneBall b;
+  b.x = (float)x; b.y = (float)y; b.z = (float)z;
+  b.r2 = __double2float_ru(rr * rr);
+  return b;
+}
+
+// does the box [bl, bh] come within the ball's radius of its centre?
+__device__ __forceinline__ bool lane_ball_hits(const LaneBall &q, const float *bl, const float *bh) {
+  const float dx = fmaxf(fmaxf(bl[0] - q.x, q.x - bh[0]), 0.f);
+  const float dy = fmaxf(fmaxf(bl[1] - q.y, q.y - bh[1]), 0.f);
+  const float dz = fmaxf(fmaxf(bl[2] - q.z, q.z - bh[2]), 0.f);
+  return dx * dx + dy * dy + dz * dz <= q.r2;
+}
+
 __device__ __forceinline__ bool lane_box_hits(const LaneBox &q, const float *bl, const float *bh) {
   return (bl[0] <= q.hi[0]) & (bh[0] >= q.lo[0]) & (bl[1] <= q.hi[1]) & (bh[1] >= q.lo[1]) & (bl[2] <= q.hi[2]) &
          (bh[2] >= q.lo[2]);
@@ -297,6 +322,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 6) k_solve_range(SolveArg
       const float thr = prefilter_threshold(pf, r);
       int c = 0;
       const LaneBox lb = lane_query_box(xi, yi, zi, r);
+      const LaneBall lball = lane_ball(xi, yi, zi, r);
       const unsigned onmask = share_lane_boxes(sm, lb, on);
       const bool any_dwalk = __any_sync(kFull, dwalk);
       stack_ok &= walk_leaves(a.t, ql, qh, sm.lbox, onmask, sm.stack, [&](int lj, const float *bl, const float *bh) {
@@ -309,7 +335,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 6) k_solve_range(SolveArg
           // FP64 d2 as t testing the leaf itself, in |targets| rounds
           // instead of 32 (a lane needs about half the leaves its warp
           // visits).
-          const unsigned tm = __ballot_sync(kFull, on && lane_box_hits(lb, bl, bh));
+          const unsigned tm = __ballot_sync(kFull, on && lane_box_hits(lb, bl, bh) && lane_ball_hits(lball, bl, bh));
           if (!tm) return;
           double xk = 1e300, yk = 1e300, zk = 1e300;  // past the last particle: never a neighbour
           if ((int)lane_id() < cntj) {
