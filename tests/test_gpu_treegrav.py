@@ -38,7 +38,10 @@ def _cloud(kind, n=20000):
 
 @pytest.mark.parametrize("kind", ["polytrope", "uniform"])
 @pytest.mark.parametrize("precision", [0, 1])
-def test_tree_gravity_error_bounds(kind, precision):
+@pytest.mark.parametrize("key_mode", [0, 1])
+def test_tree_gravity_error_bounds(kind, precision, key_mode):
+    """Also on the reference's Peano-Hilbert keys (key_mode 1): their common
+    prefixes are cells of the curve too, so the radix tree holds."""
     from cudasph_b200.simulation import Simulation, make_params
     ic = _cloud(kind)
     ref = O.gravity(ic["x"], ic["y"], ic["z"], ic["m"], ic["range"], O.make_params(soft_mode=1, eps=0.01))
@@ -46,7 +49,7 @@ def test_tree_gravity_error_bounds(kind, precision):
     errs = []
     for th, bound in BOUNDS.items():
         sim = Simulation(ic, make_params(precision=precision, n_target=50.0, soft_mode=1, eps=0.01, grav_mode=1,
-                                         theta=th))
+                                         theta=th, key_mode=key_mode))
         sim.CUDA_gravity()
         g = np.stack([sim.get(k) for k in ("gx", "gy", "gz")], 1)
         phi = sim.get("phi")
