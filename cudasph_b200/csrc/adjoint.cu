@@ -595,31 +595,29 @@ __global__ void __launch_bounds__(128) k_adj_hydro(AdjArgs a) {
     if (k >= cnt) continue;
     const int j = __ldg(lst + (size_t)k * kLeaf);
     if (j == s) continue;
-    const double4 pj = ld4(a.pos + j), vj = ld4(a.vpup + j), hj = ld4(a.hyd + j), dj = ld4(a.dd + j);
+    const double4 pj = ld4(a.pos + j), vj = ld4(a.vpup + j), fj = ld4(a.aux + j);
     const double4 abj = ld4(a.ab + j);
     const double mj = __ldg(&a.vel[j].w);
     const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
     const double dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
     const double ds = sqrt(dx * dx + dy * dy + dz * dz);
+    const double ids = ds > 0 ? 1.0 / ds : 0.0, imj = 1.0 / mj;
     const double drdv = dx * dvx + dy * dvy + dz * dvz;
     const double u = ds * ih;
-    const double pr_j = hj.y / (hj.x * hj.x);
-    const double c_j = sqrt(gam * hj.y / hj.x);
-    const double ad_j = fabs(dj.x);
-    const double b_j = ad_j / (ad_j + dj.y + 0.0001 * c_j / (0.5 * pj.w));
+    const double pr_j = fj.y, c_j = fj.x, b_j = fj.z;  // the neighbour's factors (k_hydro_prep)
     // forward
     const bool neg = drdv < 0;
     const double S = c_i + c_j, B = b_i + b_j, Q = pr_i + pr_j;
     double mu0 = 0, mu = 0, visc = 0;
     if (neg) {
-      mu0 = drdv / (S * ds);
+      mu0 = drdv * ids / S;
       mu = mu0 * B;
       visc = Q * (-alpha * mu + beta * mu * mu);
     }
     const double dwu = k_dw<double>(u), digu = k_dig<double>(u);
     const double A1 = pr_i + 0.5 * visc;
     const double K2 = pr_i * om_i + 0.5 * psi_i;
-    const double acc = A1 * dwu * ih5 - K2 / mj * digu * ih2;
+    const double acc = A1 * dwu * ih5 - K2 * imj * digu * ih2;
     const double ud = mj * A1 * dwu * ih5 - pr_i * om_i * digu * ih2;
     // output adjoints of the pair: force vector acc*d (i: -m_j, j: +m_i), and ud*drdv
     const double gx = -mj * abi.x + mi * abj.x, gy = -mj * abi.y + mi * abj.y, gz = -mj * abi.z + mi * abj.z;
@@ -630,10 +628,10 @@ __global__ void __launch_bounds__(128) k_adj_hydro(AdjArgs a) {
     // acc, ud -> A1, dwu, digu, ih5, ih2, pr_i, om_i, psi_i
     const double A1b = accb * dwu * ih5 + udb * mj * dwu * ih5;
     const double dwub = accb * A1 * ih5 + udb * mj * A1 * ih5;
-    const double digub = -accb * K2 / mj * ih2 - udb * pr_i * om_i * ih2;
+    const double digub = -accb * K2 * imj * ih2 - udb * pr_i * om_i * ih2;
     const double ih5b = accb * A1 * dwu + udb * mj * A1 * dwu;
-    const double ih2b = -accb * K2 / mj * digu - udb * pr_i * om_i * digu;
-    const double K2b = -accb / mj * digu * ih2;
+    const double ih2b = -accb * K2 * imj * digu - udb * pr_i * om_i * digu;
+    const double K2b = -accb * imj * digu * ih2;
     prb_i += K2b * om_i - udb * om_i * digu * ih2 + A1b;
     omb_i += K2b * pr_i - udb * pr_i * digu * ih2;
     psib_i += 0.5 * K2b;
@@ -650,22 +648,18 @@ __global__ void __launch_bounds__(128) k_adj_hydro(AdjArgs a) {
       bb_i += Bb;
       const double Sb = -mu0b * mu0 / S;
       cb_i += Sb;
-      drdvb += mu0b / (S * ds);
-      const double dsb_v = -mu0b * mu0 / ds;
+      drdvb += mu0b * ids / S;
+      const double dsb_v = -mu0b * mu0 * ids;
       atomicAdd(&a.prb[j], prjb);
       atomicAdd(&a.bb[j], Bb);
       atomicAdd(&a.cb[j], Sb);
-      if (ds > 0) {
-        dxb += dsb_v * dx / ds; dyb += dsb_v * dy / ds; dzb += dsb_v * dz / ds;
-      }
+      dxb += dsb_v * dx * ids; dyb += dsb_v * dy * ids; dzb += dsb_v * dz * ids;
     }
     // u = ds * ih
     const double ub = dwub * kd_dw(u) + digub * kd_dig(u);
     ihb += ub * ds;
     const double dsb = ub * ih;
-    if (ds > 0) {
-      dxb += dsb * dx / ds; dyb += dsb * dy / ds; dzb += dsb * dz / ds;
-    }
+    dxb += dsb * dx * ids; dyb += dsb * dy * ids; dzb += dsb * dz * ids;  // ids = 0 where ds = 0
     // drdv = d . dv
     dxb += drdvb * dvx; dyb += drdvb * dvy; dzb += drdvb * dvz;
     const double dvxb = drdvb * dx, dvyb = drdvb * dy, dvzb = drdvb * dz;
@@ -1015,6 +1009,9 @@ __global__ void k_adj_predict_final(AdjArgs a, int nb) {
 int adjoint_part_doubles(int n) { return 3 * ((n + kAT - 1) / kAT) + 8; }
 
 // The whole reverse sweep; src = packed gravity sources {x1, m} of the step.
+int launch_hydro_prep(int n, const double4 *pos, const double4 *hyd, const double4 *dd, double gamma, double4 *aux,
+                      cudaStream_t st);
+
 int launch_adjoint(AdjArgs a, const double4 *src, const int *mass_mixed, double eps, double G, int precision,
                    cudaStream_t st) {
   const int n = a.n;
@@ -1048,6 +1045,7 @@ int launch_adjoint(AdjArgs a, const double4 *src, const int *mass_mixed, double 
       launches++;
     }
   }
+  launches += launch_hydro_prep(a.n, a.pos, a.hyd, a.dd, a.gamma, a.aux, st);  // the neighbours' factors
   k_adj_hydro<<<warps_blocks, 128, 0, st>>>(a); launches++;
   k_adj_vsig<<<1, 32, 0, st>>>(a); launches++;
   k_adj_particle<<<nb, kAT, 0, st>>>(a); launches++;

@@ -1028,7 +1028,7 @@ extern "C" int cudasph_adjoint(sph_ctx *c) {
   a.n_ngb = c->n_ngb; a.list = c->list; a.sc = c->sc;
   a.xb = c->xb; a.vb = c->vb; a.ab = c->ab; a.vpb = c->vpb;
   a.rhob = c->rhob; a.Pb = c->Pb; a.omb = c->omb; a.psib = c->psib; a.divb = c->divb; a.curlb = c->curlb;
-  a.cb = c->cb; a.bb = c->bb; a.prb = c->prb; a.rho_ext = c->rho_ext;
+  a.cb = c->cb; a.bb = c->bb; a.prb = c->prb; a.rho_ext = c->rho_ext; a.aux = c->aux;
   a.asc = c->asc; a.part = c->apart;
   a.alpha = c->p.av_alpha; a.beta = c->p.av_beta; a.gamma = c->p.gamma; a.cn1 = c->p.cn1; a.cn2 = c->p.cn2;
   a.eos_mode = c->p.eos_mode; a.use_psi = use_psi(c->p);

@@ -81,6 +81,7 @@ struct AdjArgs {
   double4 *ab;  // abar (xyz), dubar (w)
   double4 *vpb; // vpbar (xyz), upbar (w)
   double *rhob, *Pb, *omb, *psib, *divb, *curlb, *cb, *bb, *prb;
+  double4 *aux;  // per particle {c, P / rho^2, Balsara factor, 0}, written before the hydro VJP
   const double *rho_ext;
   double *asc;  // [0] dtbar1 in  [1] dtbar0 out  [2] vsigbar  [3] istar  [4] fbar
   double *part;

@@ -273,12 +273,19 @@ int launch_pressure(int n, double4 *hyd, int eos_mode, double gamma, unsigned *f
   k_pressure<<<(n + 255) / 256, 256, 0, st>>>(n, hyd, eos_mode, gamma, flags);
   return 1;
 }
+int launch_hydro_prep(int n, const double4 *pos, const double4 *hyd, const double4 *dd, double gamma, double4 *aux,
+                      cudaStream_t st) {
+  if (n <= 0) return 0;
+  k_hydro_prep<<<(n + 255) / 256, 256, 0, st>>>(n, pos, hyd, dd, gamma, aux);
+  return 1;
+}
+
 int launch_hydro(const HydroArgs &a, cudaStream_t st) {
   if (a.leaf1 <= a.leaf0) return 0;
   // every particle's factors: a shard's pairs reach outside its own leaves
-  k_hydro_prep<<<(a.n + 255) / 256, 256, 0, st>>>(a.n, a.pos, a.hyd, a.dd, a.gamma, a.aux);
+  int launches = launch_hydro_prep(a.n, a.pos, a.hyd, a.dd, a.gamma, a.aux, st);
   k_hydro<<<((a.leaf1 - a.leaf0) * 32 + 127) / 128, 128, 0, st>>>(a);
-  return 2;
+  return launches + 1;
 }
 
 }  // namespace sph
