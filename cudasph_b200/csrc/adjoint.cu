@@ -826,9 +826,9 @@ __global__ void __launch_bounds__(128) k_adj_density(AdjArgs a) {
   const int *lst = a.list + (size_t)leaf * a.cap * kLeaf + lane;
   const double w = pi.w;
   const double i2w = w > 0 ? 2.0 / w : 0.0;
-  // forward sums
+  // forward sums: from the kept step when it recorded them, else summed again
   double R = 0, O = 0, Qs = 0, S = 0, Dv = 0, Cx = 0, Cy = 0, Cz = 0;
-  for (int k = 0; k < kmax; k++) {
+  for (int k = 0; k < (a.dsum ? 0 : kmax); k++) {
     if (k >= cnt) continue;
     const int j = __ldg(lst + (size_t)k * kLeaf);
     const double4 pj = ld4(a.pos + j), vj = ld4(a.vpup + j);
@@ -850,8 +850,18 @@ __global__ void __launch_bounds__(128) k_adj_density(AdjArgs a) {
   double Rb = 0, Ob = 0, Qb = 0, Sb = 0, Dvb = 0, Cxb = 0, Cyb = 0, Czb = 0, wb = 0;
   if (valid && w > 0 && cnt > 0) {
     const double h = 0.5 * w, h3 = h * h * h, h5 = h3 * h * h;
-    const double rho = R / h3;
-    const double div = Dv / (rho * h5);
+    double rho, div, om_k = 0, ps_k = 0;
+    if (a.dsum) {  // the forward outputs and the sums they do not determine (S and the curl vector)
+      const double4 sm4 = a.dsum[s], d4 = a.dd[s];
+      S = sm4.x; Cx = sm4.y; Cy = sm4.z; Cz = sm4.w;
+      rho = a.hyd[s].x;
+      div = d4.x;
+      om_k = d4.z;
+      ps_k = d4.w;
+    } else {
+      rho = R / h3;
+      div = Dv / (rho * h5);
+    }
     const double cm = sqrt(Cx * Cx + Cy * Cy + Cz * Cz);
     const double curl = cm / (rho * h5);
     double rhob = a.rhob[s], hb = 0;
@@ -866,7 +876,7 @@ __global__ void __launch_bounds__(128) k_adj_density(AdjArgs a) {
     rhob -= curlb * curl / rho;
     hb -= 5.0 * curlb * curl / h;
     if (S != 0) {
-      const double om = O / (h3 * S), ps = Qs / (h * S);
+      const double om = a.dsum ? om_k : O / (h3 * S), ps = a.dsum ? ps_k : Qs / (h * S);
       const double omb = a.omb[s], psb = a.psib[s];
       Ob = omb / (h3 * S);
       Sb -= omb * om / S;

@@ -118,6 +118,8 @@ struct sph_ctx {
   // adjoint (allocated on the first cudasph_set_keep(ctx, 1))
   bool keep = false, kept = false;
   double4 *pre_acc = nullptr, *xb = nullptr, *vb = nullptr, *ab = nullptr, *vpb = nullptr, *vpup = nullptr;
+  double4 *dsum = nullptr;  // the density loop's raw sums of the kept step (FP64 density only)
+  bool dsum_ok = false;
   double *rhob = nullptr, *Pb = nullptr, *omb = nullptr, *psib = nullptr, *divb = nullptr, *curlb = nullptr;
   double *cb = nullptr, *bb = nullptr, *prb = nullptr, *rho_ext = nullptr, *asc = nullptr, *apart = nullptr;
   // sharding (cudasph_set_shard): this context computes shard `rank` of
@@ -247,7 +249,7 @@ HydroArgs hydro_args(sph_ctx *c) {
   a.nleaf = c->tree.count[0];
   a.cap = c->list_cap;
   a.pos = F.pos; a.vel = F.vel; a.hyd = F.hyd; a.dd = F.dd; a.dots = F.dots; a.vsig = F.vsig;
-  a.n_ngb = c->n_ngb; a.list = c->list; a.ngb_acc = nullptr; a.aux = c->aux;
+  a.n_ngb = c->n_ngb; a.list = c->list; a.ngb_acc = nullptr; a.aux = c->aux; a.dsum = nullptr;
   a.alpha = c->p.av_alpha; a.beta = c->p.av_beta; a.gamma = c->p.gamma;
   a.use_psi = use_psi(c->p);
   a.jside = 1;
@@ -297,7 +299,7 @@ extern "C" int cudasph_destroy(sph_ctx *c) {
   cudaFree(c->tlo); cudaFree(c->thi); cudaFree(c->tgws); cudaFree(c->keys); cudaFree(c->vals); cudaFree(c->sort_scratch);
   cudaFree(c->bbox_part); cudaFree(c->box4); cudaFree(c->aux); cudaFree(c->gsrc); cudaFree(c->gh2); cudaFree(c->mass_mixed); cudaFree(c->xbuf); cudaFree(c->flags);
   cudaFree(c->sc); cudaFree(c->fin_part); cudaFree(c->flat); cudaFree(c->slot_of);
-  cudaFree(c->pre_acc); cudaFree(c->xb); cudaFree(c->vb); cudaFree(c->ab); cudaFree(c->vpb); cudaFree(c->vpup);
+  cudaFree(c->pre_acc); cudaFree(c->dsum); cudaFree(c->xb); cudaFree(c->vb); cudaFree(c->ab); cudaFree(c->vpb); cudaFree(c->vpup);
   cudaFree(c->rhob); cudaFree(c->Pb); cudaFree(c->omb); cudaFree(c->psib); cudaFree(c->divb); cudaFree(c->curlb);
   cudaFree(c->cb); cudaFree(c->bb); cudaFree(c->prb); cudaFree(c->rho_ext); cudaFree(c->asc); cudaFree(c->apart);
   for (int ph = 0; ph < SPH_NPHASES; ph++)
@@ -661,7 +663,11 @@ extern "C" int cudasph_density(sph_ctx *c) {
   SPH_CUDA_TRY(cudaSetDevice(c->device));
   PhaseScope ps(c, SPH_PH_DENSITY);
   HydroArgs a = hydro_args(c);
-  if (c->p.precision == SPH_PREC_MIXED && (c->p.mixed_sph & 1)) LAUNCHED(launch_density_mixed(a, c->st));
+  const bool fp32 = c->p.precision == SPH_PREC_MIXED && (c->p.mixed_sph & 1);
+  // a kept step records the FP64 loop's raw sums for the density VJP
+  a.dsum = (c->keep && !fp32) ? c->dsum : nullptr;
+  c->dsum_ok = a.dsum != nullptr;
+  if (fp32) LAUNCHED(launch_density_mixed(a, c->st));
   else LAUNCHED(launch_density(a, c->st));
   c->density_ok = true;
   SPH_CUDA_TRY(cudaGetLastError());
@@ -929,7 +935,7 @@ extern "C" int cudasph_set_keep(sph_ctx *c, int on) {
   if (on && !c->pre_acc) {
     const int n = c->n;
     int rc = SPH_OK;
-    double4 **d4[] = {&c->pre_acc, &c->xb, &c->vb, &c->ab, &c->vpb, &c->vpup};
+    double4 **d4[] = {&c->pre_acc, &c->xb, &c->vb, &c->ab, &c->vpb, &c->vpup, &c->dsum};
     for (double4 **p : d4)
       if (!rc) rc = dalloc(p, n);
     double **d1[] = {&c->rhob, &c->Pb, &c->omb, &c->psib, &c->divb, &c->curlb, &c->cb, &c->bb, &c->prb, &c->rho_ext};
@@ -1029,6 +1035,7 @@ extern "C" int cudasph_adjoint(sph_ctx *c) {
   a.xb = c->xb; a.vb = c->vb; a.ab = c->ab; a.vpb = c->vpb;
   a.rhob = c->rhob; a.Pb = c->Pb; a.omb = c->omb; a.psib = c->psib; a.divb = c->divb; a.curlb = c->curlb;
   a.cb = c->cb; a.bb = c->bb; a.prb = c->prb; a.rho_ext = c->rho_ext; a.aux = c->aux;
+  a.dsum = c->dsum_ok ? c->dsum : nullptr;
   a.asc = c->asc; a.part = c->apart;
   a.alpha = c->p.av_alpha; a.beta = c->p.av_beta; a.gamma = c->p.gamma; a.cn1 = c->p.cn1; a.cn2 = c->p.cn2;
   a.eos_mode = c->p.eos_mode; a.use_psi = use_psi(c->p);

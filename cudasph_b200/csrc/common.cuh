@@ -54,6 +54,7 @@ struct HydroArgs {
   const int *n_ngb, *list;
   double *ngb_acc;  // optional, list layout: m_i * acc per pair
   double4 *aux;     // per particle {c, P / rho^2, Balsara factor, 0}, written by launch_hydro
+  double4 *dsum;    // optional (kept for the adjoint): the density loop's raw sums {S, Cx, Cy, Cz}
   double alpha, beta, gamma;
   int use_psi;
   int jside;  // 1: add the j-side pair force with atomics; 0: leave it to the caller
@@ -82,6 +83,7 @@ struct AdjArgs {
   double4 *vpb; // vpbar (xyz), upbar (w)
   double *rhob, *Pb, *omb, *psib, *divb, *curlb, *cb, *bb, *prb;
   double4 *aux;  // per particle {c, P / rho^2, Balsara factor, 0}, written before the hydro VJP
+  const double4 *dsum;  // the forward density loop's raw sums {S, Cx, Cy, Cz}, or null (recomputed)
   const double *rho_ext;
   double *asc;  // [0] dtbar1 in  [1] dtbar0 out  [2] vsigbar  [3] istar  [4] fbar
   double *part;

@@ -76,6 +76,7 @@ __global__ void __launch_bounds__(128) k_density(HydroArgs a) {
     }
   }
   if (!valid) return;
+  if (a.dsum) a.dsum[s] = make_double4(sdig, cx, cy, cz);
   double4 d = make_double4(0, 0, 0, 0);
   double rho = 0;
   if (w > 0 && cnt > 0) {
