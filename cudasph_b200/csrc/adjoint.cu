@@ -1047,10 +1047,10 @@ int launch_adjoint(AdjArgs a, const double4 *src, const int *mass_mixed, double 
     launches++;
     if (nt >= 2) {
       if (precision == SPH_PREC_FP64)
-        k_adj_grav_sym_f64<<<(unsigned)sym_S(nt - 1), kAdj64Warps * 32, 0, st>>>(n, nt, src, a.ab, a.xb, eps * eps, G,
+        k_adj_grav_sym_f64<<<(unsigned)sym_items(nt), kAdj64Warps * 32, 0, st>>>(n, nt, src, a.ab, a.xb, eps * eps, G,
                                                                                   mass_mixed);
       else
-        k_adj_grav_sym_f32<<<(unsigned)sym_S(nt - 1), kAdjWarps * 32, 0, st>>>(n, nt, src, a.ab, a.xb,
+        k_adj_grav_sym_f32<<<(unsigned)sym_items(nt), kAdjWarps * 32, 0, st>>>(n, nt, src, a.ab, a.xb,
                                                                             (float)(eps * eps), G, mass_mixed);
       launches++;
     }

@@ -116,28 +116,44 @@ __device__ __forceinline__ void raise_flag(unsigned *flags, unsigned f) { atomic
 
 // Work items of the symmetric (each pair once) direct-N kernels: the Morton
 // order is cut into nt tiles; tile row b owns the nt - 1 - b tiles above the
-// diagonal, split into items of up to kSymChunk tiles, rows in order.
-constexpr int kSymChunk = 8;
-
-// S(M) = sum_{m=1..M} ceil(m / kSymChunk): items of the rows with 1..M tiles
-__host__ __device__ __forceinline__ long long sym_S(long long M) {
-  const long long q = M / kSymChunk, r = M % kSymChunk;
-  return kSymChunk * q * (q + 1) / 2 + (q + 1) * r;
+// diagonal, split into items of up to `chunk` tiles, rows in order.
+// S(M) = sum_{m=1..M} ceil(m / chunk): items of the rows with 1..M tiles
+__host__ __device__ __forceinline__ long long sym_S(long long M, int chunk) {
+  const long long q = M / chunk, r = M % chunk;
+  return chunk * q * (q + 1) / 2 + (q + 1) * r;
 }
+
+// The chunk for nt tiles: the largest of 8, 4, 2, 1 that still gives every
+// SM of the GPU four items (592 on 148 SMs), so small N fills the GPU and
+// large N keeps long items.  A pure function of nt: every kernel, launch and
+// shard computes the same one.
+constexpr long long kSymMinItems = 4 * 148;
+__host__ __device__ __forceinline__ int sym_chunk(int nt) {
+  int c = 8;
+  while (c > 1 && sym_S(nt - 1, c) < kSymMinItems) c >>= 1;
+  return c;
+}
+
 // first work item of tile row b
-__host__ __device__ __forceinline__ long long sym_first(int b, int nt) { return sym_S(nt - 1) - sym_S(nt - 1 - b); }
+__host__ __device__ __forceinline__ long long sym_first(int b, int nt, int chunk) {
+  return sym_S(nt - 1, chunk) - sym_S(nt - 1 - b, chunk);
+}
 
 // item -> (row b, j-tiles [t_lo, t_hi)), by binary search over the rows
 __device__ __forceinline__ void sym_item(long long item, int nt, int &b, int &t_lo, int &t_hi) {
+  const int chunk = sym_chunk(nt);
   int lo = 0, hi = nt - 2;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
-    if (sym_first(mid, nt) <= item) lo = mid; else hi = mid - 1;
+    if (sym_first(mid, nt, chunk) <= item) lo = mid; else hi = mid - 1;
   }
   b = lo;
-  t_lo = b + 1 + (int)(item - sym_first(b, nt)) * kSymChunk;
-  t_hi = min(t_lo + kSymChunk, nt);
+  t_lo = b + 1 + (int)(item - sym_first(b, nt, chunk)) * chunk;
+  t_hi = min(t_lo + chunk, nt);
 }
+
+// number of work items for nt tiles
+__host__ __device__ __forceinline__ long long sym_items(int nt) { return nt >= 2 ? sym_S(nt - 1, sym_chunk(nt)) : 0; }
 
 // Contiguous balanced split of [0, count) over `world` shards: shard `rank`
 // owns [count * rank / world, count * (rank + 1) / world).

@@ -398,7 +398,7 @@ __global__ void __launch_bounds__(kGThreads) k_grav_f32x2_plummer(int n, const d
 //
 // Work split: the Morton order is cut into tiles of kSymTile particles; a
 // block owns one i-tile (kSymWarps warps, kSymRP packed i-pairs per lane) and
-// one work item = up to kSymChunk j-tiles strictly above its own, so the
+// one work item = up to sym_chunk(nt) j-tiles strictly above its own, so the
 // upper triangle of tile pairs is covered once; the diagonal tiles run
 // through the one-sided kernel.  Inside a warp the j's travel: a batch of 32
 // sources, one per lane, rotates through the lanes by shuffles, each lane
@@ -713,7 +713,7 @@ int launch_gravity(int n, const double4 *src, const double *h2src, double4 *out,
   if (world > 1) cudaMemsetAsync(out, 0, sizeof(double4) * n, st);
   const double eps2 = eps * eps;
   const int nt = (n + kSymTile - 1) / kSymTile;
-  const Span items = shard_span(nt >= 2 ? sym_S(nt - 1) : 0, rank, world);
+  const Span items = shard_span(sym_items(nt), rank, world);
   int launches = 0;
   if (precision == SPH_PREC_FP64) {
     constexpr int R = 2;
