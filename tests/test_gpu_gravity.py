@@ -1,9 +1,10 @@
 """Direct-N gravity through the standalone entry point cudasph_gravity_direct.
 
 The mixed Plummer form computes each pair once above the diagonal tiles of
-1,024 particles (work items of up to 8 tiles) and the diagonal tiles
-one-sided, so the sizes below cover: a single tile, an exact tile, a ragged
-second tile, rows split over several work items with a ragged last batch.
+1,024 particles (work items of up to 8, 4, 2 or 1 tiles: the most that still
+gives four items per SM) and the diagonal tiles one-sided, so the sizes below
+cover: a single tile, an exact tile, a ragged second tile, rows split over
+several work items with a ragged last batch, and each item length.
 Reference: the FP64 oracle restatement of sph_grav_kernel.cu:14-111 (Plummer
 mode) on the same particles.
 """
@@ -72,6 +73,27 @@ def test_fp64_plummer_gravity_matches_oracle(n):
     got = _run(p, m, 0.004, 1.0, 0)
     ref = _oracle(p, m, 0.004, 1.0)
     assert np.max(np.abs(got - ref)) <= 1e-12 * np.max(np.abs(ref))
+
+
+# Item lengths by N: 20,001 (20 tiles) takes single-tile items, 65,536 (64)
+# two, 71,380 (70, ragged) four, 97,000 (95, ragged) eight.  Checked on 512
+# sampled targets against the oracle's sum over all sources.
+@pytest.mark.parametrize("n", [65536, 71380, 97000])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_gravity_item_lengths_match_oracle(n, precision):
+    p, m = _cloud(n, 11 + n)
+    got = _run(p, m, 0.004, 1.0, precision)
+    tg = np.sort(np.random.default_rng(n).choice(n, 512, replace=False)).astype(np.int32)
+    par = O.make_params(soft_mode=1, eps=0.004, G=1.0)
+    ref = np.stack(O.gravity(p[:, 0], p[:, 1], p[:, 2], m, np.zeros_like(m), par, targets=tg), 1)
+    g = got[tg]
+    assert np.all(np.isfinite(got))
+    if precision == 0:
+        assert np.max(np.abs(g - ref)) <= 1e-12 * np.max(np.abs(ref))
+    else:
+        a, r = g[:, :3], ref[:, :3]
+        assert np.sqrt(np.mean(np.sum((a - r) ** 2, 1)) / np.mean(np.sum(r ** 2, 1))) < 1e-5
+        assert np.max(np.abs(g[:, 3] / ref[:, 3] - 1)) < 1e-5
 
 
 def test_mixed_pair_forces_conserve_momentum():
