@@ -117,10 +117,23 @@ __device__ __forceinline__ void raise_flag(unsigned *flags, unsigned f) { atomic
 // Work items of the symmetric (each pair once) direct-N kernels: the Morton
 // order is cut into nt tiles; tile row b owns the nt - 1 - b tiles above the
 // diagonal, split into items of up to `chunk` tiles, rows in order.
-// S(M) = sum_{m=1..M} ceil(m / chunk): items of the rows with 1..M tiles
+// S(M) = sum_{m=1..M} ceil(m / chunk): items of the rows with 1..M tiles.
+// The chunk is one of 8, 4, 2, 1, dispatched to constants so that every
+// division is a shift (64-bit division by a runtime value is a long software
+// routine, and the item map runs it in a binary search at every block start:
+// 10 % of the 1M gravity kernel when it did).
+template <int C>
+__host__ __device__ __forceinline__ long long sym_S_c(long long M) {
+  const long long q = M / C, r = M % C;
+  return C * q * (q + 1) / 2 + (q + 1) * r;
+}
 __host__ __device__ __forceinline__ long long sym_S(long long M, int chunk) {
-  const long long q = M / chunk, r = M % chunk;
-  return chunk * q * (q + 1) / 2 + (q + 1) * r;
+  switch (chunk) {
+    case 8: return sym_S_c<8>(M);
+    case 4: return sym_S_c<4>(M);
+    case 2: return sym_S_c<2>(M);
+    default: return sym_S_c<1>(M);
+  }
 }
 
 // The chunk for nt tiles: the largest of 8, 4, 2, 1 that still gives every
@@ -134,22 +147,26 @@ __host__ __device__ __forceinline__ int sym_chunk(int nt) {
   return c;
 }
 
-// first work item of tile row b
-__host__ __device__ __forceinline__ long long sym_first(int b, int nt, int chunk) {
-  return sym_S(nt - 1, chunk) - sym_S(nt - 1 - b, chunk);
-}
-
 // item -> (row b, j-tiles [t_lo, t_hi)), by binary search over the rows
-__device__ __forceinline__ void sym_item(long long item, int nt, int &b, int &t_lo, int &t_hi) {
-  const int chunk = sym_chunk(nt);
+template <int C>
+__device__ __forceinline__ void sym_item_c(long long item, int nt, int &b, int &t_lo, int &t_hi) {
+  const long long top = sym_S_c<C>(nt - 1);
   int lo = 0, hi = nt - 2;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
-    if (sym_first(mid, nt, chunk) <= item) lo = mid; else hi = mid - 1;
+    if (top - sym_S_c<C>(nt - 1 - mid) <= item) lo = mid; else hi = mid - 1;
   }
   b = lo;
-  t_lo = b + 1 + (int)(item - sym_first(b, nt, chunk)) * chunk;
-  t_hi = min(t_lo + chunk, nt);
+  t_lo = b + 1 + (int)(item - (top - sym_S_c<C>(nt - 1 - b))) * C;
+  t_hi = min(t_lo + C, nt);
+}
+__device__ __forceinline__ void sym_item(long long item, int nt, int &b, int &t_lo, int &t_hi) {
+  switch (sym_chunk(nt)) {
+    case 8: sym_item_c<8>(item, nt, b, t_lo, t_hi); break;
+    case 4: sym_item_c<4>(item, nt, b, t_lo, t_hi); break;
+    case 2: sym_item_c<2>(item, nt, b, t_lo, t_hi); break;
+    default: sym_item_c<1>(item, nt, b, t_lo, t_hi); break;
+  }
 }
 
 // number of work items for nt tiles
