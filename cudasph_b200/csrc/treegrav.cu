@@ -33,6 +33,7 @@
 // direct kernels; larger opened nodes are pushed.  Pair terms are FP32 on
 // coordinates relative to the group's first particle (FP64 anchor); each
 // sweep's FP32 partials fold into FP64.
+#include <atomic>
 #include <cstdint>
 
 #include "common.cuh"
@@ -613,9 +614,16 @@ int launch_tree_gravity(const TreeView &t, const uint64_t *keys, const double4 *
   a.eps2 = (float)(eps * eps); a.theta = (float)theta; a.G = G;
   a.leaf0 = (int)l0; a.leaf1 = (int)l1;
   const int warps = (int)(l1 - l0);
-  static int per_sm = 0;  // resident blocks per SM (the same on every device of one architecture)
-  if (per_sm == 0 && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tree_gravity, kTgWarps * 32, 0) != cudaSuccess)
-    per_sm = 1;
+  // resident blocks per SM (the same on every device of one architecture),
+  // looked up once; contexts on several host threads may race to store it
+  static std::atomic<int> cached_per_sm{0};
+  int per_sm = cached_per_sm.load(std::memory_order_relaxed);
+  if (per_sm == 0) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tree_gravity, kTgWarps * 32, 0) != cudaSuccess ||
+        per_sm < 1)
+      per_sm = 1;
+    cached_per_sm.store(per_sm, std::memory_order_relaxed);
+  }
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
     sms = 148;
