@@ -314,7 +314,9 @@ class RefPipeline:
         n = self.n
         self.off = np.zeros(n + 1, np.int32)
         # the reference sizes lists from solve_range's count; one extra slot
-        # per particle absorbs the round-off case noted in DESIGN.md
+        # per particle absorbs the round-off case in which find_ngb's walk
+        # (dev_find_ngb.cu:67) admits one more neighbour than that count
+        # (dev_solve_range.cu:142)
         tot = ref().ref_ngb_offsets(n, self.n_ngb + 1, self.off)
         self.lst = np.full(tot, -1, np.int32)
         walk = np.zeros(n, np.int32)

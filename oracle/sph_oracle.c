@@ -12,7 +12,7 @@
  * ds2 = (dx*dx + dy*dy) + dz*dz, ds2 < range*range is bit-identical to the
  * non-contracted form the GPU kernels use.
  *
- * Deliberate departures from the reference (documented in DESIGN.md):
+ * Deliberate departures from the reference:
  *   - double instead of float everywhere (the reference device code is FP32);
  *   - the divergence/curl weight uses m_j, not m_i (dev_density_loop.cu:64 has
  *     m_i; identical for equal masses);
