@@ -112,3 +112,27 @@ def test_create_without_gpu_reports_cuda_error():
     h = C.c_void_p()
     assert L.cudasph_create(C.byref(p), 100, 0, C.byref(h)) == 1  # SPH_ERR_CUDA
     assert b"failed" in L.cudasph_last_error()
+
+
+def test_key_entries_validate_arguments_before_any_device_work():
+    """The key entry points reject bad sizes, bit counts and null buffers with
+    SPH_ERR_ARG, and return SPH_OK for n = 0, without touching a device."""
+    L = _capi.lib()
+    for bits in (0, 22, -1):
+        assert L.cudasph_peano_hilbert_keys(4, None, None, None, bits, None, None) == 2, bits
+    assert L.cudasph_peano_hilbert_keys(-1, None, None, None, 18, None, None) == 2
+    assert L.cudasph_peano_hilbert_keys(0, None, None, None, 18, None, None) == 0
+    assert L.cudasph_peano_hilbert_keys(4, None, None, None, 18, None, None) == 2
+    assert L.cudasph_peano_keys(-1, None, None, None, None, None, None) == 2
+    assert L.cudasph_peano_keys(0, None, None, None, None, None, None) == 0
+    assert L.cudasph_peano_keys(4, None, None, None, None, None, None) == 2
+    assert L.cudasph_morton_keys(4, None, None, None, None, None, None) == 2
+
+
+def test_key_mode_is_validated():
+    L = _capi.lib()
+    p = L.cudasph_default_params()
+    assert p.key_mode == 0
+    p.key_mode = 2
+    h = C.c_void_p()
+    assert L.cudasph_create(C.byref(p), 100, 0, C.byref(h)) == 2
