@@ -266,8 +266,14 @@ def adjoint_cost(steps=5, warmup=3, headline_n=None):
         sim.adjoint()
         return fwd
 
-    for name, prec in (("fp64", 0), ("mixed", 1)):
-        sim = Simulation(ic, make_params(precision=prec, **ADJOINT_PARAMS))
+    # the h solve at the reference's tolerance (rel_err 1e-3, 20 iterations: the
+    # forward step's setting) and at the tight tolerance the gradient tests use
+    # (rel_err 1e-12, 80 iterations), where the solved range is the root that
+    # the adjoint's implicit derivative of the h solve describes
+    settings = (("fp64", 0, 1e-3, 20), ("mixed", 1, 1e-3, 20),
+                ("fp64_tight_h", 0, 1e-12, 80), ("mixed_tight_h", 1, 1e-12, 80))
+    for name, prec, rel_err, max_iter in settings:
+        sim = Simulation(ic, make_params(precision=prec, rel_err=rel_err, max_iter=max_iter, **ADJOINT_PARAMS))
         sim.set_keep(True)
         m = ic["m"]
         for _ in range(warmup):  # warm-up includes the reverse sweep (first use of its kernels)
@@ -282,7 +288,8 @@ def adjoint_cost(steps=5, warmup=3, headline_n=None):
             sim.set_profiling(False)
             adj_s.append(ph["adjoint"][0])
         fwd, adj = float(np.median(fwd_s)), float(np.median(adj_s))
-        out[name] = {"forward_ms": fwd, "adjoint_ms": adj, "adjoint_over_forward": adj / fwd,
+        out[name] = {"rel_err": rel_err, "max_iter": max_iter, "forward_ms": fwd, "adjoint_ms": adj,
+                     "adjoint_over_forward": adj / fwd,
                      "replay_plus_adjoint_over_forward": (fwd + adj) / fwd, "flags": sim.device_status(),
                      "samples_forward_ms": [round(v, 3) for v in fwd_s],
                      "samples_adjoint_ms": [round(v, 3) for v in adj_s]}
@@ -301,7 +308,7 @@ def adjoint_cost(steps=5, warmup=3, headline_n=None):
         ph = sim.phase_times()
         sim.set_profiling(False)
         adj = ph["adjoint"][0]
-        out["headline_workload_mixed"] = {"n": headline_n, "forward_ms": fwd, "adjoint_ms": adj,
+        out["headline_workload_mixed"] = {"n": headline_n, "rel_err": 1e-3, "forward_ms": fwd, "adjoint_ms": adj,
                                           "adjoint_over_forward": adj / fwd,
                                           "replay_plus_adjoint_over_forward": (fwd + adj) / fwd,
                                           "flags": sim.device_status()}
@@ -533,6 +540,159 @@ def c2_run(n=C2_N, steps=50, n_grav_targets=512):
     return res
 
 
+def dropin_run(n=C2_N, steps=3):
+    """The drop-in path as a user of the reference gets it: the reference's own
+    C++ driver (its CUDAsph_iterate.cpp, step.cpp, sph_accelerations.cpp,
+    CUDA_calls.cpp, CUDA_gravity.cpp, ... compiled unmodified and linked
+    against this library in place of the reference's host_calls.cu:
+    oracle/_ref/CUDAsph_iterate_b200) on a restart file of an n-particle
+    n=1.5 polytrope (u x (1 + U(-0.05, 0.05)), mu 0.62) for `steps` steps.
+    The driver's own compiled-in parameters apply (DESIRED_NGB = 24, spline
+    softening, gas + radiation EOS).  Reported: the per-iteration wall seconds
+    the driver prints (step.cpp:137-145) and its phase lines: the host kd-tree
+    (kd_tree.cpp:97-114), the device time of the two library calls, the host
+    j-side scatter (sph_accelerations.cpp:104-115) and the gravity call
+    (CUDA_gravity.cpp:3-71); the steady figure is the median of the
+    iterations after the first (which creates the library's context)."""
+    import re
+    from cudasph_b200 import ics, state_io
+    from cudasph_b200.simulation import Simulation, make_params
+    drv = os.path.join(ROOT, "oracle", "_ref", "CUDAsph_iterate_b200")
+    if not os.path.exists(drv):
+        return {"unavailable": "oracle/_ref/CUDAsph_iterate_b200 is not built (needs the reference sources)"}
+    ic = ics.polytrope(n, n_poly=1.5, n_ngb=24.0, seed=12345 + 2, u_jitter=0.05, mu=0.62)
+    ic = {k: (v.astype(np.float32).astype(np.float64) if isinstance(v, np.ndarray) else v) for k, v in ic.items()}
+    # the driver runs while its time is below t_end: the native step under the
+    # driver's parameters gives the times after each step (the first has dt = 0)
+    sim = Simulation(ic, make_params(n_target=24.0, eos_mode=1, soft_mode=0, use_psi=1))
+    times = []
+    for _ in range(steps):
+        sim.step()
+        times.append(sim.time)
+    sim.close()
+    t_end = 0.5 * (times[-2] + times[-1]) if steps >= 2 else 1e-12
+    with tempfile.TemporaryDirectory() as d:
+        hdr = state_io.default_header(n, t_end=t_end, dt_out=0.0, dt=0.0, global_time=0.0, iteration_number=0)
+        state_io.write_state(os.path.join(d, "init.bin"), hdr, ic)
+        t0 = time.perf_counter()
+        r = subprocess.run([drv, "init.bin"], cwd=d, capture_output=True, text=True, timeout=900)
+        wall = time.perf_counter() - t0
+    if r.returncode != 0:
+        return {"error": f"driver exit {r.returncode}", "stderr_tail": r.stderr[-500:]}
+    err = r.stderr
+
+    def grab(pat):
+        return [float(v) for v in re.findall(pat, err, flags=re.S)]
+
+    num = r"([0-9.eE+-]+)"
+    it = grab(r"Iteration took " + num + " seconds")
+    res = {"workload": f"n=1.5 polytrope, N={n}, reference driver parameters (DESIRED_NGB=24, spline softening, "
+                       f"gas+radiation EOS mu=0.62)",
+           "iterations": len(it), "iteration_s": [round(v, 4) for v in it], "process_wall_s": round(wall, 2),
+           "phase_s": {"kd_tree_host": grab(r"building kd-tree \.\.\..*?done in " + num + " sec"),
+                       "device_calls": grab(r"Device was used for " + num + " seconds"),
+                       "sph_accelerations": grab(r"done SPH accelerations in " + num + " sec"),
+                       "add_ngb_acc_host": grab(r"add_ngb_acc on the host \.\.\. done in " + num + " sec"),
+                       "gravity": grab(r"Computing gravity \.\.\.\s+done in " + num + " sec")}}
+    steady = it[1:] if len(it) > 1 else it
+    if steady:
+        res["s_per_step"] = float(np.median(steady))
+        res["particle_steps_per_s"] = n / res["s_per_step"]
+    return res
+
+
+FIRST_STEP_FIELDS = ("range", "rho", "divv", "curlv", "omega", "psi", "P", "ax", "ay", "az", "du", "vsig", "gx",
+                     "gy", "gz", "phi")
+
+
+def first_step_fields(sim, order):
+    """The outputs of a step in tree order (slot s = original particle
+    order[s]); after the first step from the initial conditions (dt = 0, so
+    the predictor leaves x, v and u as they are) the forces in ax..az (hydro
+    + gravity) belong to the initial state."""
+    return {k: sim.get(k)[order] for k in FIRST_STEP_FIELDS}
+
+
+def oracle_pass(ic, first, n_grav_targets=2048, seed=0):
+    """The cpu_baseline leg: the FP64 oracle (oracle/sph_oracle.c, OpenMP over
+    all host threads) runs the force evaluation of the first step on the
+    workload's initial state with the workload's own parameters (N_ngb = 64,
+    Plummer eps = 0.002, gas + radiation EOS), in the GPU's tree order, each
+    phase timed: h solve from the same guesses, neighbour lists, density,
+    EOS, hydro with the j-side scatter over all particles; gravity for a
+    seeded sample of targets against all sources, extrapolated to all
+    targets.  The lists and everything after them are taken at the FP64 GPU
+    step's ranges, so the same pass is the checker of the GPU's first steps:
+    errors of each GPU form against the oracle (density, EOS, hydro over all
+    particles; gravity and total force over the sampled targets)."""
+    from oracle import oracle as O
+    n = ic["x"].size
+    par = O.make_params(**WORKLOAD_PARAMS)
+    order = first.get("order")
+    if order is None:
+        k, _ = O.morton_keys(ic["x"], ic["y"], ic["z"])
+        order = O.sort_order(k)
+    s = {k: np.ascontiguousarray(np.asarray(ic[k], np.float64)[order]) for k in
+         ("x", "y", "z", "range", "vx", "vy", "vz", "m", "u", "mu")}
+    t = {}
+    t0 = time.perf_counter()
+    r_o, _, _ = O.solve_range(s["x"], s["y"], s["z"], s["range"], par)
+    t["solve_range"] = time.perf_counter() - t0
+    r_gpu = first["fp64"]["range"] if "fp64" in first else r_o
+    t0 = time.perf_counter()
+    cnt, off, lst = O.find_ngb(s["x"], s["y"], s["z"], r_gpu)
+    t["find_ngb"] = time.perf_counter() - t0
+    s["range"] = r_gpu
+    t0 = time.perf_counter()
+    s.update(O.density(s, off, lst))
+    t["density"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    s["P"] = O.pressure(s["rho"], s["u"], s["mu"], par)
+    t["pressure"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    h = O.hydro(s, off, lst, par)
+    t["hydro"] = time.perf_counter() - t0
+    tg = np.sort(np.random.default_rng(seed).choice(n, n_grav_targets, replace=False)).astype(np.int32)
+    t0 = time.perf_counter()
+    g = O.gravity(s["x"], s["y"], s["z"], s["m"], r_gpu, par, targets=tg)
+    tgs = time.perf_counter() - t0
+    measured = sum(t.values()) + tgs
+    step_s = sum(t.values()) + tgs * n / n_grav_targets
+    cb = {"value": n / step_s, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
+          "config": "this workload's own parameters (N_ngb=64, Plummer eps=0.002, gas+radiation EOS mu=0.62)",
+          "sample": (f"FP64 oracle (C restatement of the reference loops, OpenMP) on the same {n}-particle initial "
+                     f"state: h solve, neighbour lists, density, EOS, hydro + j-side scatter over all {n} "
+                     f"particles; gravity for {n_grav_targets} seeded targets x {n} sources"),
+          "measured_s": round(measured, 3), "gravity_sample_s": round(tgs, 3), "gravity_targets": n_grav_targets,
+          "extrapolated": True, "extrapolation": f"gravity x {n}/{n_grav_targets}",
+          "s_per_step_extrapolated": round(step_s, 3), "phase_s": {k: round(v, 3) for k, v in t.items()}}
+    against = {}
+    if "fp64" not in first:
+        return cb, against
+    g3 = np.stack(g[:3], 1)
+    h3 = np.stack([h["ax"], h["ay"], h["az"]], 1)
+    for form, f in first.items():
+        if form == "order":
+            continue
+        a = np.stack([f["ax"], f["ay"], f["az"]], 1)
+        gg = np.stack([f["gx"], f["gy"], f["gz"]], 1)
+        e = {"h_identical_frac": float(np.mean(f["range"] == r_o)),
+             "max_rho_rel": float(np.max(np.abs(f["rho"] / s["rho"] - 1))),
+             "max_P_rel": float(np.max(np.abs(f["P"] / s["P"] - 1))),
+             "rms_hydro_rel": rms_rel(a - gg, h3),
+             "rms_du_rel": float(np.sqrt(np.mean((f["du"] - h["du"]) ** 2) / max(np.mean(h["du"] ** 2), 1e-300))),
+             "max_vsig_rel": float(np.max(np.abs(f["vsig"] / h["vsig"] - 1))),
+             "rms_gravity_rel": rms_rel(gg[tg], g3),
+             "max_phi_rel": float(np.max(np.abs(f["phi"][tg] / g[3] - 1))),
+             "rms_force_rel": rms_rel(a[tg], h3[tg] + g3)}
+        against[form] = e
+    against["note"] = (f"first step from the initial state (dt = 0); density, EOS and hydro over all {n} "
+                       f"particles at the FP64 GPU step's ranges, gravity and total force (hydro + gravity) over "
+                       f"{n_grav_targets} seeded targets; h_identical_frac: the GPU's ranges against the "
+                       f"oracle's own h solve")
+    return cb, against
+
+
 def cpu_reference_sample(ic, n_grav_targets=2048):
     from oracle import oracle as O
     if not O.ref_available():
@@ -590,7 +750,7 @@ def run_ours(args, rank, world):
     sim.close()
 
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-           "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+           "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "strong",
            "vs_baseline": None, "dtype": "f64" if args.fp64_only else "f32+f64", "data": "synthetic (seeded)",
            "config": {"workload": workload_name(n), "n_particles": n, "precision": "fp64" if args.fp64_only else
                       "mixed (FP32 gravity pair terms, FP64 SPH pair terms)", "l2": "state (~%.0f MB) larger than L2; no flush" % (n * 500 / 1e6),
@@ -618,12 +778,17 @@ def run_ours(args, rank, world):
     out["sph_roofline"] = sph_bandwidth(ph, args.steps, n, stats["ngb_mean"])
 
     # --- FP64 comparison and errors ----------------------------------------------
+    first = {}  # tree-order fields after the first step of each form (the oracle check below)
     if not args.fp64_only and args.fp64_steps > 0:
         kw64 = dict(kw, precision=0)
         s64 = Simulation(ic, make_params(**kw64), device=dev)
         s32 = Simulation(ic, make_params(**kw), device=dev)
         s64.step(1)
         s32.step(1)
+        order = s64.order()
+        first["order"] = order
+        first["fp64"] = first_step_fields(s64, order)
+        first["mixed"] = first_step_fields(s32, order)
         a64 = np.stack([s64.get(k) for k in ("ax", "ay", "az")], 1)
         a32 = np.stack([s32.get(k) for k in ("ax", "ay", "az")], 1)
         g64 = np.stack([s64.get(k) for k in ("gx", "gy", "gz")], 1)
@@ -638,12 +803,13 @@ def run_ours(args, rank, world):
                   "rms_hydro_rel": rms_rel(a32 - g32, a64 - g64),
                   "rms_force_rel_to_gravity_scale": float(np.sqrt(np.mean(np.sum((a32 - a64) ** 2, 1))
                                                                   / np.mean(np.sum(g64 ** 2, 1)))),
-                  "against": "FP64 GPU step (equal to the FP64 oracle to 1e-12 in the parity tests) at the "
-                             "same state, first step"}
+                  "against": "FP64 GPU step at the same state, first step (errors against the FP64 oracle: "
+                             "errors.against_oracle, from the cpu_baseline leg)"}
         s32.close()
         # the option with the density and hydro pair terms in FP32 as well
         s3 = Simulation(ic, make_params(**dict(kw, mixed_sph=3)), device=dev)
         s3.step(1)
+        first["mixed_sph_3"] = first_step_fields(s3, order)
         a3 = np.stack([s3.get(k) for k in ("ax", "ay", "az")], 1)
         g3 = np.stack([s3.get(k) for k in ("gx", "gy", "gz")], 1)
         errors["mixed_sph_3"] = {"rms_force_rel": rms_rel(a3, a64), "rms_hydro_rel": rms_rel(a3 - g3, a64 - g64),
@@ -689,19 +855,40 @@ def run_ours(args, rank, world):
                       "d2h_bytes_per_step": 8 * n * len(outs), "steps": args.e2e_steps,
                       "api": "cudasph_step_host (C ABI), pinned host buffers, wall clock"}
 
-    # --- CPU baseline: the reference's own code on the host ----------------------------
+    # --- energy drift over 100 steps (mixed and FP64 side by side) -----------------------
+    if args.drift_line_steps > 0:
+        out[f"drift_{args.drift_line_steps}"] = energy_drift(n, args.drift_line_steps)
+
+    # --- the drop-in path: the reference's own driver on this library ---------------------
+    if args.dropin_steps > 0:
+        di = dropin_run(steps=args.dropin_steps)
+        out["dropin"] = di
+        if "s_per_step" in di:
+            out["dropin_s_per_step"] = di["s_per_step"]
+
+    # --- CPU baseline: the FP64 oracle at this workload's own parameters (and the ------
+    # --- checker of the first steps above), the reference's own code beside it ---------
     if args.cpu_baseline:
+        cb, against = oracle_pass(ic, first, n_grav_targets=args.cpu_grav_targets)
         r = cpu_reference_sample(ic, n_grav_targets=args.cpu_grav_targets)
         if r is not None:
             t, cores = r
-            out["cpu_baseline"] = {
+            cb["reference_build"] = {
                 "value": n / t["step"], "unit": UNIT, "cores": cores, "kind": "reference",
+                "config": "reference compiled-in: DESIRED_NGB=24, spline softening (not this workload's "
+                          "N_ngb=64 / Plummer eps=0.002; its sources are compiled unmodified)",
                 "sample": (f"reference device code + kd-tree built for the CPU (oracle/_ref), one step on the "
-                           f"same {n}-particle state: kd-tree build, solve_range, find_ngb, density, pressure, "
-                           f"hydro + scatter over all particles, gravity for {args.cpu_grav_targets} sampled "
-                           f"targets x {n} sources extrapolated to {n}; the reference's compiled-in "
-                           f"DESIRED_NGB=24 and spline softening"),
+                           f"same {n}-particle initial state: kd-tree build, solve_range, find_ngb, density, "
+                           f"pressure, hydro + scatter over all particles, gravity for {args.cpu_grav_targets} "
+                           f"sampled targets x {n} sources"),
+                "measured_s": round(sum(v for k, v in t.items() if k not in ("step", "gravity")), 3),
+                "gravity_sample_s": round(t["gravity_sample"], 3), "gravity_targets": args.cpu_grav_targets,
+                "extrapolated": True, "extrapolation": f"gravity x {n}/{args.cpu_grav_targets}",
+                "s_per_step_extrapolated": round(t["step"], 3),
                 "phase_s": {k: round(v, 3) for k, v in t.items()}}
+        out["cpu_baseline"] = cb
+        if against and "errors" in out:
+            out["errors"]["against_oracle"] = against
     return out
 
 
@@ -807,6 +994,13 @@ def run_sharded(args, rank, world):
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the reference's own CPU implementation of the path
+    (its device loops and kd-tree compiled for the host, oracle/_ref), on the
+    same initial state, each step a bounded sample: the whole SPH pass over
+    all particles plus the gravity of args.cpu_grav_targets seeded targets,
+    the gravity extrapolated to all targets.  The FP64 oracle at this
+    workload's own parameters is timed once beside it (the reference's
+    sources fix DESIRED_NGB = 24 and spline softening)."""
     if rank != 0:
         return None
     from oracle import oracle as O
@@ -814,23 +1008,36 @@ def run_reference(args, rank, world):
         return {"impl": "reference", "unavailable": "oracle/_ref (the reference built for the host CPU) is missing"}
     n = args.n
     ic = workload_ic(n)
-    times = []
+    times, measured, grav_s = [], [], []
+    t_wall = time.perf_counter()
     for i in range(args.warmup + args.steps):
         R = O.RefPipeline(ic)
         t = R.time_step(n_grav_targets=args.cpu_grav_targets, seed=i)
         if i >= args.warmup:
             times.append(t["step"])
+            measured.append(sum(v for k, v in t.items() if k not in ("step", "gravity")))
+            grav_s.append(t["gravity_sample"])
+    wall = time.perf_counter() - t_wall
     ms = 1000.0 * float(np.mean(times))
     value = n * 1000.0 / ms
     cores = O.ref().ref_num_threads()
+    same_cfg, _ = oracle_pass(ic, {}, n_grav_targets=args.cpu_grav_targets)
     return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)", "impl": "reference",
-            "config": {"workload": workload_name(n), "n_particles": n, "precision": "reference FP32 + float-float"},
+            "config": {"workload": workload_name(n), "n_particles": n,
+                       "precision": "reference FP32 + float-float",
+                       "reference_parameters": "compiled-in DESIRED_NGB=24 and spline softening"},
+            "timing": {"ms_per_step": "extrapolated: measured SPH pass + gravity sample x N/targets",
+                       "measured_s_per_step": round(float(np.mean(measured)) + float(np.mean(grav_s)), 3),
+                       "gravity_sample_s": round(float(np.mean(grav_s)), 3),
+                       "gravity_targets": args.cpu_grav_targets, "extrapolated": True,
+                       "wall_s_all_steps": round(wall, 1)},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
                              "sample": f"per step: full SPH pass over {n} particles with the reference's code "
                                        f"(DESIRED_NGB=24, spline softening), gravity on {args.cpu_grav_targets} "
                                        f"sampled targets x {n} sources extrapolated"},
+            "oracle_same_config": same_cfg,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -860,6 +1067,10 @@ def main():
     # all particles, about 6 s of CPU work per sampled step at N = 1M on 16 threads
     ap.add_argument("--cpu-grav-targets", type=int, default=2048)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--drift-line-steps", type=int, default=100,
+                    help="energy drift over this many steps of the mixed and FP64 forms in the bench line (0: skip)")
+    ap.add_argument("--dropin-steps", type=int, default=3,
+                    help="steps of the reference's own driver on this library (N = 262,144; 0: skip)")
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false")
     ap.add_argument("--no-tree", dest="tree", action="store_false",
                     help="skip the tree-gravity measurement (opt-in Barnes-Hut mode)")

@@ -54,6 +54,9 @@ sph_ctx *g_ctx = nullptr;
 int g_n = 0;
 double *g_acc = nullptr;  // ngb_acc in list layout (FP64)
 size_t g_acc_cap = 0;
+double4 *g_grav_src = nullptr, *g_grav_out = nullptr;  // compute_CUDA_gravity's sources and results
+double *g_grav_h2 = nullptr;
+size_t g_grav_cap = 0;
 
 sph_ctx *legacy_ctx(int n_real) {
   if (g_ctx && g_n == n_real) return g_ctx;
@@ -212,19 +215,25 @@ void zcopyArrayToDevice(float *device, const float *host, int numBodies, int) {
 
 void compute_CUDA_gravity(int numBodies, sph_legacy_float4 *accel, float *pos, float *vel, int, int, int) {
   if (numBodies <= 0) return;
-  double4 *src = nullptr, *out = nullptr;
-  double *h2 = nullptr;
-  check(cudaMalloc((void **)&src, sizeof(double4) * numBodies), "cudaMalloc");
-  check(cudaMalloc((void **)&out, sizeof(double4) * numBodies), "cudaMalloc");
-  check(cudaMalloc((void **)&h2, sizeof(double) * numBodies), "cudaMalloc");
+  // FP64 sources and results live in buffers kept across calls (grown when a
+  // call has more bodies), so a driver step allocates nothing here
+  if ((size_t)numBodies > g_grav_cap) {
+    cudaFree(g_grav_src);
+    cudaFree(g_grav_out);
+    cudaFree(g_grav_h2);
+    g_grav_src = g_grav_out = nullptr;
+    g_grav_h2 = nullptr;
+    check(cudaMalloc((void **)&g_grav_src, sizeof(double4) * numBodies), "cudaMalloc");
+    check(cudaMalloc((void **)&g_grav_out, sizeof(double4) * numBodies), "cudaMalloc");
+    check(cudaMalloc((void **)&g_grav_h2, sizeof(double) * numBodies), "cudaMalloc");
+    g_grav_cap = (size_t)numBodies;
+  }
   const int nb = (numBodies + 255) / 256;
-  k_grav_in<<<nb, 256>>>(numBodies, (const float4 *)pos, (const float4 *)vel, src, h2);
-  launch_gravity(numBodies, src, h2, out, SPH_SOFT_SPLINE, 0.0, 1.0, SPH_PREC_FP64, nullptr, 0, 1, 0);
-  k_grav_out<<<nb, 256>>>(numBodies, out, (float4 *)accel);
+  k_grav_in<<<nb, 256>>>(numBodies, (const float4 *)pos, (const float4 *)vel, g_grav_src, g_grav_h2);
+  launch_gravity(numBodies, g_grav_src, g_grav_h2, g_grav_out, SPH_SOFT_SPLINE, 0.0, 1.0, SPH_PREC_FP64, nullptr, 0,
+                 1, 0);
+  k_grav_out<<<nb, 256>>>(numBodies, g_grav_out, (float4 *)accel);
   check(cudaDeviceSynchronize(), "get_CUDA_forces");
-  cudaFree(src);
-  cudaFree(out);
-  cudaFree(h2);
 }
 
 float host_solve_range(int n_bodies, int n_nodes, float rel_err, sph_legacy_kv *bodies_hash, int *bodies_map,

@@ -449,27 +449,76 @@ static __device__ __align__(256) unsigned char g_noalloc_sort_scratch[kNoAllocSc
 
 }  // namespace sph
 
+#include <cuda.h>  // driver types only; the entry points come from cudaGetDriverEntryPoint
+
 #include <mutex>
 
 namespace {
 // Host code cannot use the array's name as a device address (on the host it
-// names a stand-in object), so the address is looked up once per device with
-// that device current and cached.
+// names a stand-in object), so the address is looked up with the device
+// current and cached per device, together with the id of the context it was
+// looked up in: after a cudaDeviceReset the library's module is loaded again
+// into a new primary context, the array may move, and the next call looks the
+// address up anew.
 constexpr int kMaxDevices = 128;
 std::mutex g_noalloc_mu;
-void *g_noalloc_ptr[kMaxDevices] = {};
+struct NoAllocSlot {
+  void *ptr;
+  unsigned long long ctx_id;
+};
+NoAllocSlot g_noalloc[kMaxDevices] = {};
+
+typedef CUresult (*ctx_get_current_fn)(CUcontext *);
+typedef CUresult (*ctx_get_id_fn)(CUcontext, unsigned long long *);
+
+ctx_get_current_fn g_get_current = nullptr;
+ctx_get_id_fn g_get_id = nullptr;
+
+// whether the driver gives context ids (resolved once)
+bool context_ids_available() {
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *f = nullptr, *g = nullptr;
+    cudaDriverEntryPointQueryResult q1, q2;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q1) == cudaSuccess &&
+        cudaGetDriverEntryPoint("cuCtxGetId", &g, cudaEnableDefault, &q2) == cudaSuccess &&
+        q1 == cudaDriverEntryPointSuccess && q2 == cudaDriverEntryPointSuccess) {
+      g_get_current = (ctx_get_current_fn)f;
+      g_get_id = (ctx_get_id_fn)g;
+    }
+    (void)cudaGetLastError();
+  });
+  return g_get_current && g_get_id;
+}
+
+// id of the context current on this thread, 0 if none is
+unsigned long long current_context_id() {
+  CUcontext c = nullptr;
+  unsigned long long id = 0;
+  if (g_get_current(&c) != CUDA_SUCCESS || !c || g_get_id(c, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
 
 int noalloc_scratch(void **out) {
   int dev = 0;
   SPH_CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kMaxDevices) return SPH_ERR_ARG;
+  if (dev < 0 || dev >= kMaxDevices) {
+    sph_internal_set_error("cudasph_radix_sort_u64_noalloc: device ordinal beyond the address cache");
+    return SPH_ERR_ARG;
+  }
+  // without context ids from the driver the address is cached per device only
+  const bool ids = context_ids_available();
+  const unsigned long long ctx = ids ? current_context_id() : 0;
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
+  NoAllocSlot &slot = g_noalloc[dev];
+  if (!slot.ptr || (ids && slot.ctx_id != ctx)) {
     void *p = nullptr;
     SPH_CUDA_TRY(cudaGetSymbolAddress(&p, sph::g_noalloc_sort_scratch));
-    g_noalloc_ptr[dev] = p;
+    slot.ptr = p;
+    // the lookup made the device's context current if none was
+    slot.ctx_id = ids ? current_context_id() : 0;
   }
-  *out = g_noalloc_ptr[dev];
+  *out = slot.ptr;
   return SPH_OK;
 }
 }  // namespace
@@ -482,7 +531,10 @@ extern "C" int cudasph_radix_sort_u64_noalloc(int n, uint64_t *keys, uint32_t *v
     sph_internal_set_error(msg);
     return SPH_ERR_ARG;
   }
-  if (n > 0 && (!keys || !vals)) return SPH_ERR_ARG;
+  if (n > 0 && (!keys || !vals)) {
+    sph_internal_set_error("cudasph_radix_sort_u64_noalloc: keys and vals must be device pointers (null given)");
+    return SPH_ERR_ARG;
+  }
   if (n <= 1) return SPH_OK;
   void *scratch = nullptr;
   int rc = noalloc_scratch(&scratch);

@@ -619,14 +619,22 @@ int launch_tree_gravity(const TreeView &t, const uint64_t *keys, const double4 *
   static std::atomic<int> cached_per_sm{0};
   int per_sm = cached_per_sm.load(std::memory_order_relaxed);
   if (per_sm == 0) {
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tree_gravity, kTgWarps * 32, 0) != cudaSuccess ||
-        per_sm < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tree_gravity, kTgWarps * 32, 0) == cudaSuccess &&
+        per_sm >= 1) {
+      cached_per_sm.store(per_sm, std::memory_order_relaxed);
+    } else {
+      // a failed query is neither cached nor left pending: the caller's
+      // post-launch error check must only see the launch's own status
+      (void)cudaGetLastError();
       per_sm = 1;
-    cached_per_sm.store(per_sm, std::memory_order_relaxed);
+    }
   }
   int dev = 0, sms = 148;
-  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    (void)cudaGetLastError();
     sms = 148;
+  }
   const int blocks = min((warps + kTgWarps - 1) / kTgWarps, sms * max(per_sm, 1));
   cudaMemsetAsync(w.next_group, 0, sizeof(unsigned), st);
   k_tree_gravity<<<blocks, kTgWarps * 32, 0, st>>>(a);

@@ -293,7 +293,10 @@ int cudasph_peano_keys(int n, const double *x, const double *y, const double *z,
  * n returns SPH_ERR_ARG with a message.  No cudaMalloc, cudaFree or other
  * allocating routine is called.  The first call on a device looks up the
  * array's device address on that device (cudaGetSymbolAddress), so make that
- * first call outside any stream capture.  All calls share the one array and
+ * first call outside any stream capture; the first call after a
+ * cudaDeviceReset of that device looks it up again (the array moves with the
+ * reloaded library module), so make that one outside capture too.  Null
+ * keys or vals with n > 1 return SPH_ERR_ARG with a message.  All calls share the one array and
  * nothing in it needs to start at zero, but calls whose GPU work overlaps
  * (two streams, or two host threads) race on it: serialise them. */
 #define CUDASPH_SORT_NOALLOC_MAX_KEYS 262144

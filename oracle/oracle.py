@@ -81,6 +81,12 @@ def lib():
     L.orc_quartic_root.restype = C.c_double
     L.orc_hydro.argtypes = [C.c_int] + [_dp] * 14 + [_lp, _ip] + [_dp] * 5 + [C.c_void_p, C.POINTER(OrcParams)]
     L.orc_gravity.argtypes = [C.c_int, C.c_void_p, C.c_int] + [_dp] * 9 + [C.POINTER(OrcParams)]
+    L.orc_solve_range_tgt.argtypes = [C.c_int, _ip, C.c_int, _dp, _dp, _dp, _dp, _dp, _ip, _ip,
+                                      C.POINTER(OrcParams)]
+    L.orc_find_ngb_tgt.argtypes = [C.c_int, _ip, C.c_int, _dp, _dp, _dp, _dp, _ip, _lp, C.c_void_p]
+    L.orc_find_ngb_tgt.restype = C.c_longlong
+    L.orc_density_tgt.argtypes = [C.c_int, _ip] + [_dp] * 8 + [_lp, _ip] + [_dp] * 5
+    L.orc_hydro_tgt.argtypes = [C.c_int, _ip, C.c_int] + [_dp] * 14 + [_dp] * 5 + [C.POINTER(OrcParams)]
     L.orc_morton_keys.argtypes = [C.c_int, _dp, _dp, _dp, _up, C.c_void_p]
     L.orc_peano_keys.argtypes = [C.c_int, _dp, _dp, _dp, _up, C.c_void_p]
     L.orc_peano_hilbert_key.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int]
@@ -177,6 +183,58 @@ def gravity(x, y, z, m, rng, params: OrcParams, targets=None):
     g = [np.zeros(nt) for _ in range(4)]
     lib().orc_gravity(nt, tp, n, x, y, z, m, rng, *g, C.byref(params))
     return g
+
+
+# ---------------------------------------------------------------------------
+# the same loops for a sample of target particles against the whole state
+# (parity checks at the full workload sizes)
+# ---------------------------------------------------------------------------
+def _tgt(targets):
+    return np.ascontiguousarray(targets, np.int32)
+
+
+def solve_range_sample(x, y, z, range0, targets, params: OrcParams):
+    """h solve of the targets only (all particles are candidates), each from
+    its guess range0[target]: (range, n_ngb, evaluations) per target."""
+    x, y, z, r0, t = _f64(x), _f64(y), _f64(z), _f64(range0), _tgt(targets)
+    rng = np.zeros(t.size)
+    nn = np.zeros(t.size, np.int32)
+    ne = np.zeros(t.size, np.int32)
+    lib().orc_solve_range_tgt(t.size, t, x.size, x, y, z, r0, rng, nn, ne, C.byref(params))
+    return rng, nn, ne
+
+
+def find_ngb_sample(x, y, z, range_t, targets):
+    """Exact lists {j : ds2 < range_t[t]^2} (ascending j) of the targets, as
+    CSR over the targets."""
+    x, y, z, rt, t = _f64(x), _f64(y), _f64(z), _f64(range_t), _tgt(targets)
+    cnt = np.zeros(t.size, np.int32)
+    off = np.zeros(t.size + 1, np.int64)
+    tot = lib().orc_find_ngb_tgt(t.size, t, x.size, x, y, z, rt, cnt, off, None)
+    lst = np.zeros(max(tot, 1), np.int32)
+    lib().orc_find_ngb_tgt(t.size, t, x.size, x, y, z, rt, cnt, off, lst.ctypes.data_as(C.c_void_p))
+    return cnt, off, lst[:tot]
+
+
+def density_sample(s: dict, targets, off, lst):
+    """Density loop of the targets over their lists (find_ngb_sample's CSR)."""
+    t = _tgt(targets)
+    out = {k: np.zeros(t.size) for k in ("rho", "divv", "curlv", "omega", "psi")}
+    lib().orc_density_tgt(t.size, t, *[_f64(s[k]) for k in ("x", "y", "z", "range", "vx", "vy", "vz", "m")],
+                          np.ascontiguousarray(off, np.int64), np.ascontiguousarray(lst, np.int32),
+                          out["rho"], out["divv"], out["curlv"], out["omega"], out["psi"])
+    return out
+
+
+def hydro_sample(s: dict, targets, params: OrcParams):
+    """Hydro derivatives of the targets, i-side and j-side, over the whole
+    state s (per-particle fields of every particle taken as given)."""
+    t = _tgt(targets)
+    out = {k: np.zeros(t.size) for k in ("ax", "ay", "az", "du", "vsig")}
+    lib().orc_hydro_tgt(t.size, t, s["x"].size, *[_f64(s[k]) for k in (
+        "x", "y", "z", "range", "vx", "vy", "vz", "m", "rho", "P", "divv", "curlv", "omega", "psi")],
+        out["ax"], out["ay"], out["az"], out["du"], out["vsig"], C.byref(params))
+    return out
 
 
 def morton_keys(x, y, z):

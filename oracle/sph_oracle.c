@@ -339,13 +339,16 @@ static double solve_range_one(cand_list *cl, double w, const orc_params *p, int 
   return w;
 }
 
-/* dev_solve_range kernel, dev_solve_range.cu:174-189: range <- solution for
- * every particle with range > 0.  n_ngb is the hard count at the final range. */
-void orc_solve_range(int n, const double *x, const double *y, const double *z, double *range,
-                     int *n_ngb, int *nevals_out, const orc_params *p) {
-  if (n <= 0) return;
+/* dev_solve_range kernel, dev_solve_range.cu:174-189, for targets tgt[0..nt)
+ * (NULL: every particle, t = i): range_out[t] <- the solution started from
+ * range_in[i], over all n particles as candidates (ascending index), for every
+ * target with range > 0.  n_ngb[t] is the hard count at the final range. */
+static void solve_targets(int nt, const int *tgt, int n, const double *x, const double *y, const double *z,
+                          const double *range_in, double *range_out, int *n_ngb, int *nevals_out,
+                          const orc_params *p) {
+  if (n <= 0 || nt <= 0) return;
   double cell = 0;
-  for (int i = 0; i < n; i++) cell += range[i];
+  for (int i = 0; i < n; i++) cell += range_in[i];
   cell = cell / n;
   if (!(cell > 0)) cell = 1;
   orc_grid g;
@@ -356,9 +359,10 @@ void orc_solve_range(int n, const double *x, const double *y, const double *z, d
     memset(&cl, 0, sizeof(cl));
     cl.g = &g; cl.x = x; cl.y = y; cl.z = z;
 #pragma omp for schedule(dynamic, 64)
-    for (int i = 0; i < n; i++) {
+    for (int t = 0; t < nt; t++) {
+      const int i = tgt ? tgt[t] : t;
       int ne = 0;
-      double w = range[i];
+      double w = range_in[i];
       if (w > 0) {
         cl.xi = x[i]; cl.yi = y[i]; cl.zi = z[i];
         cl.nc = -1; cl.R = -1;
@@ -366,18 +370,32 @@ void orc_solve_range(int n, const double *x, const double *y, const double *z, d
         double f, dx, cnt;
         cand_ensure(&cl, w);
         compute_ngb(cl.d2, cl.nc, w, p, &f, &dx, &cnt);
-        n_ngb[i] = (int)cnt;
+        n_ngb[t] = (int)cnt;
       } else {
         w = 0;
-        n_ngb[i] = 0;
+        n_ngb[t] = 0;
       }
-      range[i] = w;
-      if (nevals_out) nevals_out[i] = ne;
+      range_out[t] = w;
+      if (nevals_out) nevals_out[t] = ne;
     }
     free(cl.buf);
     free(cl.d2);
   }
   grid_free(&g);
+}
+
+/* every particle, range updated in place */
+void orc_solve_range(int n, const double *x, const double *y, const double *z, double *range,
+                     int *n_ngb, int *nevals_out, const orc_params *p) {
+  solve_targets(n, NULL, n, x, y, z, range, range, n_ngb, nevals_out, p);
+}
+
+/* a sample of targets (the full-size parity checks): range_out, n_ngb and
+ * nevals_out have nt entries */
+void orc_solve_range_tgt(int nt, const int *tgt, int n, const double *x, const double *y, const double *z,
+                         const double *range0, double *range_out, int *n_ngb, int *nevals_out,
+                         const orc_params *p) {
+  solve_targets(nt, tgt, n, x, y, z, range0, range_out, n_ngb, nevals_out, p);
 }
 
 /* ------------------------------------------------------------------ */
@@ -426,18 +444,55 @@ long long orc_find_ngb(int n, const double *x, const double *y, const double *z,
   return offsets[n];
 }
 
+/* find_ngb for targets tgt[0..nt) at ranges range_t[t] (exact sets over all n
+ * particles, ascending index).  Same two-call protocol as orc_find_ngb:
+ * list == NULL fills counts and offsets (nt + 1 entries). */
+long long orc_find_ngb_tgt(int nt, const int *tgt, int n, const double *x, const double *y, const double *z,
+                           const double *range_t, int *counts, long long *offsets, int *list) {
+  if (n <= 0 || nt <= 0) { if (offsets) offsets[0] = 0; return 0; }
+  double cell = 0;
+  for (int t = 0; t < nt; t++) cell += range_t[t];
+  cell = cell / nt;
+  if (!(cell > 0)) cell = 1;
+  orc_grid g;
+  grid_build(&g, n, x, y, z, cell);
+#pragma omp parallel
+  {
+    int cap = 0, *buf = NULL;
+    double *db = NULL;
+#pragma omp for schedule(dynamic, 16)
+    for (int t = 0; t < nt; t++) {
+      const int i = tgt[t];
+      int c = range_t[t] > 0 ? grid_query(&g, x, y, z, x[i], y[i], z[i], range_t[t], &buf, &cap, &db) : 0;
+      counts[t] = c;
+      if (list) memcpy(list + offsets[t], buf, sizeof(int) * c);
+    }
+    free(buf); free(db);
+  }
+  grid_free(&g);
+  if (!list) {
+    long long tot = 0;
+    for (int t = 0; t < nt; t++) { offsets[t] = tot; tot += counts[t]; }
+    offsets[nt] = tot;
+  }
+  return offsets[nt];
+}
+
 /* ------------------------------------------------------------------ */
 /* Density loop: dev_density_loop.cu:29-86                              */
 /* ------------------------------------------------------------------ */
-void orc_density(int n, const double *x, const double *y, const double *z, const double *range,
-                 const double *vx, const double *vy, const double *vz, const double *m,
-                 const long long *offsets, const int *list,
-                 double *rho, double *divv, double *curlv, double *omega, double *psi) {
+/* targets tgt[0..nt) (NULL: every particle, t = i); list t at offsets[t],
+ * outputs at t */
+static void density_targets(int nt, const int *tgt, const double *x, const double *y, const double *z,
+                            const double *range, const double *vx, const double *vy, const double *vz,
+                            const double *m, const long long *offsets, const int *list,
+                            double *rho, double *divv, double *curlv, double *omega, double *psi) {
 #pragma omp parallel for schedule(dynamic, 64)
-  for (int i = 0; i < n; i++) {
+  for (int t = 0; t < nt; t++) {
+    const int i = tgt ? tgt[t] : t;
     double dens = 0, om = 0, ps = 0, sdig = 0, div = 0, cx = 0, cy = 0, cz = 0;
     double w = range[i];
-    for (long long k = offsets[i]; k < offsets[i + 1]; k++) {
+    for (long long k = offsets[t]; k < offsets[t + 1]; k++) {
       int j = list[k];
       double dx = x[i] - x[j], dy = y[i] - y[j], dz = z[i] - z[j];
       double u = 2 * sqrt(ds2_of(dx, dy, dz)) / w;
@@ -453,7 +508,7 @@ void orc_density(int n, const double *x, const double *y, const double *z, const
       cz += wt * (dx * dvy - dy * dvx);
     }
     double h = 0.5 * w;
-    if (w > 0 && offsets[i + 1] > offsets[i]) {
+    if (w > 0 && offsets[t + 1] > offsets[t]) {
       double h3 = h * h * h, h5 = h3 * h * h;
       if (sdig != 0) {
         om *= 1.0 / h3 / sdig;
@@ -464,11 +519,26 @@ void orc_density(int n, const double *x, const double *y, const double *z, const
       dens *= 1.0 / h3;
       div *= 1.0 / dens / h5;
       double c = sqrt(cx * cx + cy * cy + cz * cz) / dens / h5;
-      rho[i] = dens; divv[i] = div; curlv[i] = c; omega[i] = om; psi[i] = ps;
+      rho[t] = dens; divv[t] = div; curlv[t] = c; omega[t] = om; psi[t] = ps;
     } else {
-      rho[i] = 0; divv[i] = 0; curlv[i] = 0; omega[i] = 0; psi[i] = 0;
+      rho[t] = 0; divv[t] = 0; curlv[t] = 0; omega[t] = 0; psi[t] = 0;
     }
   }
+}
+
+void orc_density(int n, const double *x, const double *y, const double *z, const double *range,
+                 const double *vx, const double *vy, const double *vz, const double *m,
+                 const long long *offsets, const int *list,
+                 double *rho, double *divv, double *curlv, double *omega, double *psi) {
+  density_targets(n, NULL, x, y, z, range, vx, vy, vz, m, offsets, list, rho, divv, curlv, omega, psi);
+}
+
+/* a sample of targets: lists and outputs indexed by t (orc_find_ngb_tgt's CSR) */
+void orc_density_tgt(int nt, const int *tgt, const double *x, const double *y, const double *z,
+                     const double *range, const double *vx, const double *vy, const double *vz, const double *m,
+                     const long long *offsets, const int *list,
+                     double *rho, double *divv, double *curlv, double *omega, double *psi) {
+  density_targets(nt, tgt, x, y, z, range, vx, vy, vz, m, offsets, list, rho, divv, curlv, omega, psi);
 }
 
 /* ------------------------------------------------------------------ */
@@ -610,6 +680,81 @@ void orc_hydro(int n, const double *x, const double *y, const double *z, const d
     }
   }
   if (!ngb_acc) free(nacc);
+}
+
+/* orc_hydro's result for targets tgt[0..nt) over the whole state, each pair
+ * found by scanning all n particles in ascending index:
+ *   i-side, dev_hydro_dots.cu:25-84: every j with ds2 < range_i^2 (i's own
+ *     list, in list order), giving a_i, du_i and vsig_i;
+ *   j-side, sph_accelerations.cpp:106-114: every j with ds2 < range_j^2 (i is
+ *     in j's list), adding m_j acc_ji (x_j - x_i), acc_ji evaluated with j as
+ *     the list owner exactly as the i-side loop does for its own pairs.
+ * The per-particle inputs (range, rho, P, div v, curl v, omega, psi) of all n
+ * are taken as given: this checks the hydro loop on a sample of a state whose
+ * per-particle fields are checked separately. */
+void orc_hydro_tgt(int nt, const int *tgt, int n, const double *x, const double *y, const double *z,
+                   const double *range, const double *vx, const double *vy, const double *vz, const double *m,
+                   const double *rho, const double *P, const double *divv, const double *curlv,
+                   const double *omega, const double *psi,
+                   double *ax, double *ay, double *az, double *du, double *vsig, const orc_params *p) {
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int t = 0; t < nt; t++) {
+    const int i = tgt[t];
+    double axi = 0, ayi = 0, azi = 0, udot = 0, vmax = 0;
+    double sx = 0, sy = 0, sz = 0; /* j-side, summed apart and added at the end */
+    const double hi = 0.5 * range[i];
+    const double prho2 = (rho[i] > 0) ? P[i] / (rho[i] * rho[i]) : 0;
+    const double h2 = hi * hi, h5 = h2 * h2 * hi;
+    const double psi_i = p->use_psi ? psi[i] : 0;
+    const double ri2 = range[i] * range[i];
+    for (int j = 0; j < n; j++) {
+      const double dx = x[i] - x[j], dy = y[i] - y[j], dz = z[i] - z[j];
+      const double d2 = ds2_of(dx, dy, dz);
+      const int own = d2 < ri2, other = d2 < range[j] * range[j];
+      if (!own && !other) continue;
+      const double dvx = vx[i] - vx[j], dvy = vy[i] - vy[j], dvz = vz[i] - vz[j];
+      const double ds = sqrt(d2);
+      const double drdv = dx * dvx + dy * dvy + dz * dvz;
+      if (own) {
+        double visc, vs;
+        art_visc(range[i], range[j], ds, drdv, rho[i], P[i], divv[i], curlv[i], rho[j], P[j], divv[j],
+                 curlv[j], p, &visc, &vs);
+        if (vs > vmax) vmax = vs;
+        const double u = ds / hi;
+        const double dwu = orc_dw(u), digu = orc_dig(u);
+        double acc = (prho2 + 0.5 * visc) * dwu / h5;
+        acc -= (prho2 * omega[i] + 0.5 * psi_i) / m[j] * digu / h2;
+        axi -= m[j] * acc * dx;
+        ayi -= m[j] * acc * dy;
+        azi -= m[j] * acc * dz;
+        double ud = m[j] * (prho2 + 0.5 * visc) * dwu / h5;
+        ud -= prho2 * omega[i] * digu / h2;
+        udot += ud * drdv;
+      }
+      if (other) {
+        /* the pair (j, i) of j's list: the same expressions with j as owner */
+        const double ex = x[j] - x[i], ey = y[j] - y[i], ez = z[j] - z[i];
+        const double evx = vx[j] - vx[i], evy = vy[j] - vy[i], evz = vz[j] - vz[i];
+        const double eds = sqrt(ds2_of(ex, ey, ez));
+        const double edrdv = ex * evx + ey * evy + ez * evz;
+        const double hj = 0.5 * range[j];
+        const double prho2j = (rho[j] > 0) ? P[j] / (rho[j] * rho[j]) : 0;
+        const double hj2 = hj * hj, hj5 = hj2 * hj2 * hj;
+        const double psi_j = p->use_psi ? psi[j] : 0;
+        double visc, vs;
+        art_visc(range[j], range[i], eds, edrdv, rho[j], P[j], divv[j], curlv[j], rho[i], P[i], divv[i],
+                 curlv[i], p, &visc, &vs);
+        const double u = eds / hj;
+        double acc = (prho2j + 0.5 * visc) * orc_dw(u) / hj5;
+        acc -= (prho2j * omega[j] + 0.5 * psi_j) / m[i] * orc_dig(u) / hj2;
+        const double a = m[j] * acc;
+        sx += a * ex;
+        sy += a * ey;
+        sz += a * ez;
+      }
+    }
+    ax[t] = axi + sx; ay[t] = ayi + sy; az[t] = azi + sz; du[t] = udot; vsig[t] = vmax;
+  }
 }
 
 /* ------------------------------------------------------------------ */

@@ -136,3 +136,21 @@ def test_key_mode_is_validated():
     p.key_mode = 2
     h = C.c_void_p()
     assert L.cudasph_create(C.byref(p), 100, 0, C.byref(h)) == 2
+
+
+def test_noalloc_sort_validates_arguments_before_any_device_work():
+    """The allocation-free sort rejects a negative size, a size above its
+    fixed scratch and null buffers (with a message), and returns SPH_OK for
+    n = 0 and n = 1 without touching the buffers (the sentinel addresses
+    given here are never dereferenced), all without a device."""
+    L = _capi.lib()
+    f = L.cudasph_radix_sort_u64_noalloc
+    f.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    assert f(-1, None, None, None) == 2
+    assert f(262144 + 1, None, None, None) == 2
+    assert b"262144" in L.cudasph_last_error()
+    assert f(0, None, None, None) == 0
+    assert f(1, 0x10, 0x20, None) == 0
+    assert f(2, None, 0x20, None) == 2
+    assert b"null" in L.cudasph_last_error()
+    assert f(2, 0x10, None, None) == 2

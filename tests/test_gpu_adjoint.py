@@ -97,9 +97,9 @@ def test_adjoint_dense_reference_n4096(precision, tol, equal):
         st = T.step(st, p)
     Ld = T.loss_ke_density(st, probes)
     Ld.backward()
-    assert _rel(gx, x0.grad.cpu().numpy()) < tol
-    assert _rel(gv, v0.grad.cpu().numpy()) < tol
-    assert _rel(gu, u0.grad.cpu().numpy()) < tol
+    rel = [_rel(gx, x0.grad.cpu().numpy()), _rel(gv, v0.grad.cpu().numpy()), _rel(gu, u0.grad.cpu().numpy())]
+    print("dense n4096 precision", precision, "equal", equal, "rel", rel)
+    assert max(rel) < tol, rel
     del st, Ld
     torch.cuda.empty_cache()
 

@@ -33,12 +33,17 @@ def _keys(n, seed):
 
 
 def test_noalloc_sort_matches_allocating_sort_twice():
+    """Two calls in a row (different sizes, the second at the maximum) equal
+    the allocating sort bit for bit, and the values are the oracle's stable
+    order of the keys."""
     import torch
+    from oracle import oracle as O
     L = _lib()
     dev = torch.device("cuda:0")
     stream = torch.cuda.current_stream().cuda_stream
     for call, (n, seed) in enumerate([(100_003, 1), (MAX_KEYS, 2)]):
-        k = torch.from_numpy(_keys(n, seed)).to(dev)
+        keys = _keys(n, seed)
+        k = torch.from_numpy(keys).to(dev)
         v = torch.arange(n, dtype=torch.int32, device=dev)
         k_ref, v_ref = k.clone(), v.clone()
         scratch = torch.empty(L.cudasph_sort_scratch_bytes(n), dtype=torch.uint8, device=dev)
@@ -49,6 +54,26 @@ def test_noalloc_sort_matches_allocating_sort_twice():
         assert torch.equal(v, v_ref), f"call {call}: values differ"
         kk = k.cpu().numpy().view(np.uint64)
         assert np.all(kk[1:] >= kk[:-1])
+        assert np.array_equal(v.cpu().numpy(), O.sort_order(keys.view(np.uint64))), f"call {call}: not stable"
+
+
+def test_noalloc_sort_allocates_no_device_memory():
+    """After a first call (the address lookup), a call at the maximum size
+    leaves the device's free memory unchanged: the scratch is the array
+    compiled into the library, not an allocation."""
+    import torch
+    L = _lib()
+    dev = torch.device("cuda:0")
+    k = torch.from_numpy(_keys(MAX_KEYS, 3)).to(dev)
+    v = torch.arange(MAX_KEYS, dtype=torch.int32, device=dev)
+    assert L.cudasph_radix_sort_u64_noalloc(MAX_KEYS, k.data_ptr(), v.data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(dev)
+    for _ in range(3):
+        assert L.cudasph_radix_sort_u64_noalloc(MAX_KEYS, k.data_ptr(), v.data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(dev)
+    assert free1 == free0
 
 
 def test_noalloc_sort_rejects_more_keys_than_its_scratch():
