@@ -592,7 +592,7 @@ def dropin_run(n=C2_N, steps=3):
            "phase_s": {"kd_tree_host": grab(r"building kd-tree \.\.\..*?done in " + num + " sec"),
                        "device_calls": grab(r"Device was used for " + num + " seconds"),
                        "sph_accelerations": grab(r"done SPH accelerations in " + num + " sec"),
-                       "add_ngb_acc_host": grab(r"add_ngb_acc on the host \.\.\. done in " + num + " sec"),
+                       "add_ngb_acc_host": grab(r"add_ngb_acc on the host \.\.\.\s+done in " + num + " sec"),
                        "gravity": grab(r"Computing gravity \.\.\.\s+done in " + num + " sec")}}
     steady = it[1:] if len(it) > 1 else it
     if steady:

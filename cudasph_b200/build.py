@@ -2,9 +2,9 @@
 
 Usage: ``python -m cudasph_b200.build`` (or ``__graft_entry__.build()``).
 The library lands in ``cudasph_b200/_lib/``; object files in
-``cudasph_b200/_build/``.  Translation units that carry the FP64 h solve,
-neighbour predicate and density/hydro sums are compiled with ``-fmad=false``
-so they perform the same IEEE operations as an FP64 CPU evaluation.
+``cudasph_b200/_build/``.  The translation unit of the FP64 h solve and
+neighbour predicate is compiled with ``-fmad=false`` so it performs the same
+IEEE operations as an FP64 CPU evaluation.
 """
 from __future__ import annotations
 
@@ -23,8 +23,9 @@ LIB = os.path.join(LIBDIR, "libcudasph_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
           "-I" + os.path.join(HERE, "..", "include")]
-# no FMA contraction: results reproducible against an FP64 CPU evaluation
-NO_FMAD = {"neighbours.cu", "hydro.cu"}
+# no FMA contraction: the h solve's ranges and neighbour sets reproduce an FP64
+# CPU evaluation bit for bit
+NO_FMAD = {"neighbours.cu"}
 SOURCES = ["sort.cu", "tree.cu", "neighbours.cu", "hydro.cu", "hydro_mixed.cu", "gravity.cu", "integrate.cu",
            "capi.cu", "legacy.cu", "peak.cu", "adjoint.cu", "treegrav.cu"]
 

@@ -1019,8 +1019,8 @@ __global__ void k_adj_predict_final(AdjArgs a, int nb) {
 int adjoint_part_doubles(int n) { return 3 * ((n + kAT - 1) / kAT) + 8; }
 
 // The whole reverse sweep; src = packed gravity sources {x1, m} of the step.
-int launch_hydro_prep(int n, const double4 *pos, const double4 *hyd, const double4 *dd, double gamma, double4 *aux,
-                      cudaStream_t st);
+int launch_hydro_prep(int n, const double4 *pos, const double4 *vel, const double4 *hyd, const double4 *dd,
+                      double gamma, double4 *aux, cudaStream_t st);
 
 int launch_adjoint(AdjArgs a, const double4 *src, const int *mass_mixed, double eps, double G, int precision,
                    cudaStream_t st) {
@@ -1055,7 +1055,7 @@ int launch_adjoint(AdjArgs a, const double4 *src, const int *mass_mixed, double 
       launches++;
     }
   }
-  launches += launch_hydro_prep(a.n, a.pos, a.hyd, a.dd, a.gamma, a.aux, st);  // the neighbours' factors
+  launches += launch_hydro_prep(a.n, a.pos, a.vel, a.hyd, a.dd, a.gamma, a.aux, st);  // the neighbours' factors
   k_adj_hydro<<<warps_blocks, 128, 0, st>>>(a); launches++;
   k_adj_vsig<<<1, 32, 0, st>>>(a); launches++;
   k_adj_particle<<<nb, kAT, 0, st>>>(a); launches++;

@@ -243,6 +243,7 @@ struct SolveArgs {
   double *dcache;  // squared distances of the cached candidates, layout of list
   int cap;
   int leaf0, leaf1;  // leaves processed by this launch
+  int speculate;     // first evaluation by a walk at the range itself (see k_solve_range)
 };
 
 enum { kBr0 = 0, kBr1 = 1, kSolve = 2, kDone = 3 };
@@ -305,6 +306,173 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 6) k_solve_range(SolveArg
   double w_list = -1.0;     // direct lanes: range of the list last written
   int cnt_list = 0;
   bool pending = false;
+  // One evaluation's epilogue (compute_ngb, dev_solve_range.cu:77-87) and
+  // the step of the lane's iteration to its next evaluation or the end.
+  auto advance = [&](double sf, double sg) {
+    nev++;
+    f = sf - a.n_target;
+    sg *= 1.0 / w;
+    if (sg != 0) dx = f / sg;
+    else dx = (f < 0) ? -w : +w;
+    bool to_solve_init = false, to_br_check = false, to_solve_check = false;
+    if (phase == kBr0 || phase == kBr1) {
+      if (fabs(dx) < rel * w) {
+        rx = w - 0.5 * fabs(dx);
+        ry = w + 0.5 * fabs(dx);
+        to_solve_init = true;
+      } else {
+        if (fabs(dx) > fs * w) dx = (dx < 0) ? -fs * w : fs * w;
+        if (phase == kBr0) {
+          x_left = w;
+          f_try = f;
+          iter = 0;
+        }
+        to_br_check = true;
+      }
+    } else {  // kSolve
+      if (f < 0) rx = w;
+      else ry = w;
+      keep = fabs(dx) > rel * w;
+      to_solve_check = true;
+    }
+    if (to_br_check) {
+      if ((f_try * f >= 0) && (iter++ < a.max_iter)) {
+        x_left = w;
+        f_try = f;
+        w -= dx;
+        phase = kBr1;
+      } else {
+        if (x_left < w) { rx = x_left; ry = w; }
+        else { rx = w; ry = x_left; }
+        to_solve_init = true;
+      }
+    }
+    if (to_solve_init) {
+      w = 0.5 * (rx + ry);
+      dx = 0;
+      if (fabs(rx - ry) > rel * w) {
+        iter = 0;
+        keep = 1;
+        to_solve_check = true;
+      } else {
+        phase = kDone;
+      }
+    }
+    if (to_solve_check) {
+      if (keep && (iter++ < a.max_iter)) {
+        w -= dx;
+        if ((w - ry) * (w - rx) >= 0) {
+          dx = 0.5 * (ry - rx);
+          w = 0.5 * (rx + ry);
+        }
+        phase = kSolve;
+      } else {
+        if (keep) raise_flag(a.flags, SPH_FLAG_H_NOT_CONVERGED);
+        phase = kDone;
+      }
+    }
+  };
+  // Speculative first evaluation.  In steady state the previous step's range
+  // (after the predictor) already passes the tolerance test for almost every
+  // particle, so the first evaluation is also the last: the warp walks the
+  // tree once at the ranges themselves, every hit (d2 < w^2) goes straight to
+  // its lane's list (index only), and each lane evaluates f and f' over its
+  // list in list order -- ascending index, the order of the walk and of the
+  // CPU loop -- recomputing the FP64 d2 of each entry from the positions (the
+  // same operations as the walk, so the same value).  No candidate cache is
+  // written or read.  A lane done after this evaluation keeps the list when
+  // its final range (w = (rx + ry) / 2, within a few ulp of the evaluated one)
+  // leaves the set unchanged: every entry inside the final range (the largest
+  // d2 checked), and, if the range grew, no candidate in the sliver just
+  // outside the evaluated range (flagged during the walk).  Otherwise the
+  // lane lists by a walk at its final range; lanes not done continue with the
+  // candidate cache below.
+  int spec_cnt = -1;  // >= 0: the speculative list is this lane's final list
+  if (a.speculate && __any_sync(kFull, phase != kDone)) {
+    const bool on = phase != kDone;
+    const double w_eval = w;
+    const double r2 = __dmul_rn(w, w);
+    const double r2hi = r2 * (1.0 + 0x1p-40);  // the sliver [w^2, r2hi)
+    const double rw = w * (1.0 + 1e-12);       // boxes and ball cover the sliver
+    float ql[3], qh[3];
+    warp_query_box(on, xi, yi, zi, rw, ql, qh);
+    const LaneBox lb = lane_query_box(xi, yi, zi, rw);
+    const LaneBall lball = lane_ball(xi, yi, zi, rw);
+    const unsigned onmask = share_lane_boxes(sm, lb, on);
+    int c = 0;
+    bool sliver = false;
+    stack_ok &= walk_leaves(a.t, ql, qh, sm.lbox, onmask, sm.stack, [&](int lj, const float *bl, const float *bh) {
+      const int cntj = min(kLeaf, n - lj * kLeaf);
+      const unsigned tm = __ballot_sync(kFull, on && lane_box_hits(lb, bl, bh) && lane_ball_hits(lball, bl, bh));
+      if (!tm) return;
+      double xk = 1e300, yk = 1e300, zk = 1e300;  // past the last particle: never a neighbour
+      if ((int)lane_id() < cntj) {
+        const double4 p = ld4(a.pos + lj * kLeaf + (int)lane_id());
+        xk = p.x; yk = p.y; zk = p.z;
+      }
+      const int jk = lj * kLeaf + (int)lane_id();
+      const unsigned below = (1u << lane_id()) - 1u;
+      unsigned m = tm;
+      while (m) {  // two targets per round, as in the cache fill below
+        const int t0 = __ffs(m) - 1;
+        m &= m - 1u;
+        const int t1 = m ? __ffs(m) - 1 : t0;
+        const bool two = m != 0u;
+        m &= m - 1u;
+        const double r20 = __shfl_sync(kFull, r2, t0), r21 = __shfl_sync(kFull, r2, t1);
+        const double s20 = __shfl_sync(kFull, r2hi, t0), s21 = __shfl_sync(kFull, r2hi, t1);
+        const double d20 = ds2_exact(sm.tx[t0] - xk, sm.ty[t0] - yk, sm.tz[t0] - zk);
+        const double d21 = ds2_exact(sm.tx[t1] - xk, sm.ty[t1] - yk, sm.tz[t1] - zk);
+        const bool h0 = d20 < r20, h1 = two && d21 < r21;
+        const unsigned hm0 = __ballot_sync(kFull, h0), hm1 = __ballot_sync(kFull, h1);
+        const unsigned sm0 = __ballot_sync(kFull, !h0 && d20 < s20), sm1 = __ballot_sync(kFull, two && !h1 && d21 < s21);
+        const int b0 = __shfl_sync(kFull, c, t0), b1 = __shfl_sync(kFull, c, t1);
+        if (h0) {
+          const int idx = b0 + __popc(hm0 & below);
+          if (idx < cap) a.list[colbase + (size_t)idx * kLeaf + (size_t)t0] = jk;
+        }
+        if (h1) {
+          const int idx = b1 + __popc(hm1 & below);
+          if (idx < cap) a.list[colbase + (size_t)idx * kLeaf + (size_t)t1] = jk;
+        }
+        if ((int)lane_id() == t0) { c += __popc(hm0); sliver |= sm0 != 0u; }
+        if ((int)lane_id() == t1) { c += __popc(hm1); sliver |= sm1 != 0u; }  // t1 != t0 whenever hm1 | sm1 != 0
+      }
+    });
+    if (on && c <= cap) {
+      double sf = 0, sg = 0, dmax = -1.0;
+      for (int k0 = 0; k0 < c; k0 += kEvalBatch) {
+        int j[kEvalBatch];
+#pragma unroll
+        for (int q = 0; q < kEvalBatch; q++) j[q] = k0 + q < c ? lst[(size_t)(k0 + q) * kLeaf] : -1;
+        double4 pj[kEvalBatch];
+#pragma unroll
+        for (int q = 0; q < kEvalBatch; q++) pj[q] = j[q] >= 0 ? ld4(a.pos + j[q]) : make_double4(xi, yi, zi, 0);
+#pragma unroll
+        for (int q = 0; q < kEvalBatch; q++) {
+          if (j[q] >= 0) {
+            const double d2 = ds2_exact(xi - pj[q].x, yi - pj[q].y, zi - pj[q].z);
+            const double u = 2 * sqrt(d2) / w;
+            sf += k_ig<double>(u);
+            sg -= k_digdh<double>(u);
+            dmax = fmax(dmax, d2);
+          }
+        }
+      }
+      advance(sf, sg);
+      if (phase == kDone) {
+        const double wf2 = __dmul_rn(w, w);
+        const bool same = (w == w_eval) || (w < w_eval && dmax < wf2) || (w > w_eval && !sliver && wf2 < r2hi);
+        if (same) {
+          spec_cnt = c;
+          cnt_list = c;
+        } else {
+          direct = true;  // list by a walk at the final range
+          pending = true;
+        }
+      }
+    }
+  }
   while (true) {
     const bool iterate = phase != kDone;
     if (!__any_sync(kFull, iterate || pending)) break;
@@ -433,70 +601,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 6) k_solve_range(SolveArg
       evaluated = true;
     }
     if (!evaluated) continue;
-    nev++;
-    // compute_ngb epilogue, dev_solve_range.cu:77-87
-    f = sf - a.n_target;
-    sg *= 1.0 / w;
-    if (sg != 0) dx = f / sg;
-    else dx = (f < 0) ? -w : +w;
-    // advance this lane's iteration to its next evaluation (or the end)
-    bool to_solve_init = false, to_br_check = false, to_solve_check = false;
-    if (phase == kBr0 || phase == kBr1) {
-      if (fabs(dx) < rel * w) {
-        rx = w - 0.5 * fabs(dx);
-        ry = w + 0.5 * fabs(dx);
-        to_solve_init = true;
-      } else {
-        if (fabs(dx) > fs * w) dx = (dx < 0) ? -fs * w : fs * w;
-        if (phase == kBr0) {
-          x_left = w;
-          f_try = f;
-          iter = 0;
-        }
-        to_br_check = true;
-      }
-    } else {  // kSolve
-      if (f < 0) rx = w;
-      else ry = w;
-      keep = fabs(dx) > rel * w;
-      to_solve_check = true;
-    }
-    if (to_br_check) {
-      if ((f_try * f >= 0) && (iter++ < a.max_iter)) {
-        x_left = w;
-        f_try = f;
-        w -= dx;
-        phase = kBr1;
-      } else {
-        if (x_left < w) { rx = x_left; ry = w; }
-        else { rx = w; ry = x_left; }
-        to_solve_init = true;
-      }
-    }
-    if (to_solve_init) {
-      w = 0.5 * (rx + ry);
-      dx = 0;
-      if (fabs(rx - ry) > rel * w) {
-        iter = 0;
-        keep = 1;
-        to_solve_check = true;
-      } else {
-        phase = kDone;
-      }
-    }
-    if (to_solve_check) {
-      if (keep && (iter++ < a.max_iter)) {
-        w -= dx;
-        if ((w - ry) * (w - rx) >= 0) {
-          dx = 0.5 * (ry - rx);
-          w = 0.5 * (rx + ry);
-        }
-        phase = kSolve;
-      } else {
-        if (keep) raise_flag(a.flags, SPH_FLAG_H_NOT_CONVERGED);
-        phase = kDone;
-      }
-    }
+    advance(sf, sg);
     if (phase == kDone) {
       if (direct) {
         pending = w != w_list;
@@ -506,7 +611,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 6) k_solve_range(SolveArg
       }
     }
   }
-  if (valid && !direct && cache_r2 >= 0) {
+  if (valid && !direct && cache_r2 >= 0 && spec_cnt < 0) {
     // the final list: the cached entries inside the final range, in order
     const double w2 = __dmul_rn(w, w);
     int c = 0;
@@ -609,6 +714,9 @@ int launch_solve_range(const TreeView &t, double4 *pos, int *nevals, unsigned *f
   a.n_ngb = n_ngb; a.list = list; a.dcache = dcache; a.cap = cap;
   a.n_target = p.n_target; a.rel_err = p.rel_err; a.f_scale = p.f_scale; a.max_iter = p.max_iter;
   a.leaf0 = leaf0; a.leaf1 = leaf1;
+  // the speculative first evaluation pays when the previous range is likely
+  // to pass the tolerance test already (not with a tight tolerance)
+  a.speculate = p.rel_err >= 1e-8;
   const int warps = leaf1 - leaf0;
   if (warps <= 0) return 0;
   k_solve_range<<<(warps + kWarpsPerBlock - 1) / kWarpsPerBlock, kWarpsPerBlock * 32, 0, st>>>(a);

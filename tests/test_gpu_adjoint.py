@@ -76,12 +76,13 @@ def test_adjoint_matches_dense_torch_autograd():
 
 
 @pytest.mark.parametrize("equal", [True, False])
-@pytest.mark.parametrize("precision,tol", [(0, 1e-7), (1, 5e-3)])
+@pytest.mark.parametrize("precision,tol", [(0, 1e-7), (1, 7e-7)])
 def test_adjoint_dense_reference_n4096(precision, tol, equal):
     """The dense O(N^2) FP64 autograd reference at N = 4096 (two steps); the
-    mixed form differentiates FP32 gravity / SPH pair terms and is held to a
-    looser bound.  Equal masses run the equal-mass form of the symmetric
-    gravity VJP, unequal masses the general form."""
+    mixed form differentiates FP32 gravity pair terms and is held to ten
+    times its measured largest gap (7.0e-8 on a B200; FP64: 9.8e-13).  Equal
+    masses run the equal-mass form of the symmetric gravity VJP, unequal
+    masses the general form."""
     from oracle import torch_dense as T
     n, K = 4096, 2
     ic = _ic(n, 8)
