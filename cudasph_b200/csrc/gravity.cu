@@ -471,7 +471,9 @@ __device__ __forceinline__ void sym_plummer_item(long long item, int n, int nt, 
     f32x2 px[kSymRP], py[kSymRP], pz[kSymRP], pp[kSymRP];
 #pragma unroll
     for (int p = 0; p < kSymRP; p++) px[p] = py[p] = pz[p] = pp[p] = 0ull;
-#pragma unroll 1
+    // two source steps per iteration: the tail of one (its shuffles) overlaps
+    // the head of the next (N = 1M: 315.7 -> 314.8 ms)
+#pragma unroll 2
     for (int s = 0; s < 32; s++) {
       const f32x2 XJ = pk2(xj, xj), YJ = pk2(yj, yj), ZJ = pk2(zj, zj), MJ = pk2(mj, mj);
       f32x2 AX = pk2(ajx, 0.f), AY = pk2(ajy, 0.f), AZ = pk2(ajz, 0.f), AP = pk2(ajp, 0.f);
