@@ -149,7 +149,7 @@ __host__ __device__ __forceinline__ int sym_chunk(int nt) {
 
 // item -> (row b, j-tiles [t_lo, t_hi)), by binary search over the rows
 template <int C>
-__device__ __forceinline__ void sym_item_c(long long item, int nt, int &b, int &t_lo, int &t_hi) {
+__host__ __device__ __forceinline__ void sym_item_c(long long item, int nt, int &b, int &t_lo, int &t_hi) {
   const long long top = sym_S_c<C>(nt - 1);
   int lo = 0, hi = nt - 2;
   while (lo < hi) {
@@ -160,7 +160,7 @@ __device__ __forceinline__ void sym_item_c(long long item, int nt, int &b, int &
   t_lo = b + 1 + (int)(item - (top - sym_S_c<C>(nt - 1 - b))) * C;
   t_hi = min(t_lo + C, nt);
 }
-__device__ __forceinline__ void sym_item(long long item, int nt, int &b, int &t_lo, int &t_hi) {
+__host__ __device__ __forceinline__ void sym_item(long long item, int nt, int &b, int &t_lo, int &t_hi) {
   switch (sym_chunk(nt)) {
     case 8: sym_item_c<8>(item, nt, b, t_lo, t_hi); break;
     case 4: sym_item_c<4>(item, nt, b, t_lo, t_hi); break;

@@ -704,6 +704,36 @@ static Span shard_span(long long count, int rank, int world) {
   return sp;
 }
 
+// The direct-N work of one launch, and of shard `rank` of `world`: one-sided
+// blocks of `block` particles -- each against the sources of its own tile of
+// `tile` particles (the diagonal tiles), or against all sources when tile is
+// 0 -- and the symmetric work items above the diagonal (tile pairs, each
+// pair once).  Shards take contiguous shares of both lists.  Host code; the
+// launch below and cudasph_gravity_plan both use it.
+struct GravPlan {
+  int tile;      // particles per symmetric tile; 0: the one-sided blocks cover all pairs
+  int block;     // particles per one-sided block
+  int nt;        // tiles
+  int chunk;     // tiles per work item
+  Span blocks;   // this shard's one-sided blocks
+  Span items;    // this shard's symmetric work items
+};
+
+static GravPlan grav_plan(int n, int soft_mode, int precision, int rank, int world) {
+  GravPlan g;
+  g.nt = (n + kSymTile - 1) / kSymTile;
+  g.chunk = g.nt >= 2 ? sym_chunk(g.nt) : 1;
+  const bool sym = soft_mode == SPH_SOFT_PLUMMER;  // the spline kernels are one-sided over all pairs
+  // FP64: R = 2 particles per thread; mixed Plummer: one packed i-pair per
+  // thread (measured fastest at N = 1M: 68 registers, more resident warps to
+  // cover the MUFU latency); mixed spline: R = 4
+  g.block = precision == SPH_PREC_FP64 ? kGThreads * 2 : (sym ? kGThreads * 2 : kGThreads * 4);
+  g.tile = sym && g.nt >= 2 ? kSymTile : 0;
+  g.blocks = shard_span((n + g.block - 1) / g.block, rank, world);
+  g.items = sym ? shard_span(sym_items(g.nt), rank, world) : Span{0, 0};
+  return g;
+}
+
 // src = {x, y, z, m} per particle; h2src = range^2 (spline mode only).
 // Shard `rank` of `world` (world > 1) computes its contiguous share of the
 // one-sided blocks (diagonal tiles, or all pairs for small n / spline
@@ -714,18 +744,17 @@ int launch_gravity(int n, const double4 *src, const double *h2src, double4 *out,
   if (n <= 0) return 0;
   if (world > 1) cudaMemsetAsync(out, 0, sizeof(double4) * n, st);
   const double eps2 = eps * eps;
-  const int nt = (n + kSymTile - 1) / kSymTile;
-  const Span items = shard_span(sym_items(nt), rank, world);
+  const GravPlan g = grav_plan(n, soft_mode, precision, rank, world);
+  const int nt = g.nt;
+  const Span &blocks = g.blocks, &items = g.items;
   int launches = 0;
   if (precision == SPH_PREC_FP64) {
     constexpr int R = 2;
     static_assert(kSymTile % (kGThreads * R) == 0, "diagonal tiles must hold whole blocks");
-    const Span blocks = shard_span((n + kGThreads * R - 1) / (kGThreads * R), rank, world);
     if (soft_mode == SPH_SOFT_PLUMMER) {
       // diagonal tiles one-sided (all pairs when there is a single tile), then the items above them
-      const int tile = nt < 2 ? 0 : kSymTile;
       if (!blocks.empty()) {
-        k_grav_f64<SPH_SOFT_PLUMMER, R><<<blocks.grid(), kGThreads, 0, st>>>(n, src, h2src, out, eps2, G, tile,
+        k_grav_f64<SPH_SOFT_PLUMMER, R><<<blocks.grid(), kGThreads, 0, st>>>(n, src, h2src, out, eps2, G, g.tile,
                                                                             (int)blocks.lo);
         launches++;
       }
@@ -740,15 +769,11 @@ int launch_gravity(int n, const double4 *src, const double *h2src, double4 *out,
     }
   } else {
     if (soft_mode == SPH_SOFT_PLUMMER) {
-      // one i-pair per thread measured fastest at N = 1M (68 registers, more
-      // resident warps to cover the MUFU latency)
       constexpr int RP = 1;
       static_assert(kSymTile % (kGThreads * 2 * RP) == 0, "diagonal tiles must hold whole blocks");
-      const Span blocks = shard_span((n + kGThreads * 2 * RP - 1) / (kGThreads * 2 * RP), rank, world);
       // diagonal tiles store, the symmetric items add on top
-      const int tile = nt < 2 ? 0 : kSymTile;
       if (!blocks.empty()) {
-        k_grav_f32x2_plummer<RP><<<blocks.grid(), kGThreads, 0, st>>>(n, src, out, (float)eps2, G, tile,
+        k_grav_f32x2_plummer<RP><<<blocks.grid(), kGThreads, 0, st>>>(n, src, out, (float)eps2, G, g.tile,
                                                                      (int)blocks.lo);
         launches++;
       }
@@ -759,7 +784,6 @@ int launch_gravity(int n, const double4 *src, const double *h2src, double4 *out,
       }
     } else {
       constexpr int R = 4;
-      const Span blocks = shard_span((n + kGThreads * R - 1) / (kGThreads * R), rank, world);
       if (!blocks.empty()) {
         k_grav_f32<SPH_SOFT_SPLINE, R><<<blocks.grid(), kGThreads, 0, st>>>(n, src, h2src, out, (float)eps2, G,
                                                                            (int)blocks.lo);
@@ -817,5 +841,30 @@ extern "C" int cudasph_gravity_direct(int n, const double *pos4, const double *r
   sph::launch_gravity(n, (const double4 *)pos4, h2, (double4 *)out4, soft_mode, eps, G, precision, nullptr, 0, 1, st);
   if (h2) SPH_CUDA_TRY(cudaFreeAsync(h2, st));
   SPH_CUDA_TRY(cudaGetLastError());
+  return SPH_OK;
+}
+
+// The gravity work plan without a device (the sharding's host-side logic).
+extern "C" int cudasph_gravity_plan(int n, int precision, int soft_mode, int rank, int world, long long *out8) {
+  if (n < 0 || !out8 || world < 1 || rank < 0 || rank >= world) return SPH_ERR_ARG;
+  if (precision != SPH_PREC_FP64 && precision != SPH_PREC_MIXED) return SPH_ERR_ARG;
+  if (soft_mode != SPH_SOFT_SPLINE && soft_mode != SPH_SOFT_PLUMMER) return SPH_ERR_ARG;
+  const sph::GravPlan g = sph::grav_plan(n, soft_mode, precision, rank, world);
+  out8[0] = g.tile;
+  out8[1] = g.block;
+  out8[2] = g.blocks.lo;
+  out8[3] = g.blocks.hi;
+  out8[4] = g.items.lo;
+  out8[5] = g.items.hi;
+  out8[6] = g.nt;
+  out8[7] = g.chunk;
+  return SPH_OK;
+}
+
+extern "C" int cudasph_gravity_item(int n, long long item, int *row, int *t_lo, int *t_hi) {
+  if (n < 0 || !row || !t_lo || !t_hi) return SPH_ERR_ARG;
+  const int nt = (n + sph::kSymTile - 1) / sph::kSymTile;
+  if (item < 0 || item >= sph::sym_items(nt)) return SPH_ERR_ARG;
+  sph::sym_item(item, nt, *row, *t_lo, *t_hi);
   return SPH_OK;
 }

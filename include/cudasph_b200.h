@@ -302,6 +302,19 @@ int cudasph_peano_keys(int n, const double *x, const double *y, const double *z,
 #define CUDASPH_SORT_NOALLOC_MAX_KEYS 262144
 int cudasph_radix_sort_u64_noalloc(int n, uint64_t *keys, uint32_t *vals, void *stream);
 
+/* The direct-N gravity work of shard `rank` of `world` for n particles at
+ * `precision` / `soft_mode` (host only, no device): out8[0] = particles per
+ * symmetric tile (0: the one-sided blocks cover every pair), [1] = particles
+ * per one-sided block, [2..3] = the shard's one-sided blocks [lo, hi) (each
+ * block's particles against the sources of their own tile, or against all
+ * sources when the tile is 0), [4..5] = its symmetric work items [lo, hi),
+ * [6] = tiles, [7] = tiles per item.  No counterpart in the reference (one
+ * GPU, CUDA_gravity.cpp:3-71). */
+int cudasph_gravity_plan(int n, int precision, int soft_mode, int rank, int world, long long *out8);
+/* symmetric work item -> i-tile `row` and j-tiles [t_lo, t_hi) above it;
+ * every pair of distinct tiles belongs to exactly one item (host only) */
+int cudasph_gravity_item(int n, long long item, int *row, int *t_lo, int *t_hi);
+
 /* direct-N gravity of n sources on themselves: pos4 = {x,y,z,m}, range =
  * smoothing ranges (spline mode), out4 = {gx,gy,gz,phi}; double buffers. */
 int cudasph_gravity_direct(int n, const double *pos4, const double *range, double *out4, int soft_mode,

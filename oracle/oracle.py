@@ -81,6 +81,7 @@ def lib():
     L.orc_quartic_root.restype = C.c_double
     L.orc_hydro.argtypes = [C.c_int] + [_dp] * 14 + [_lp, _ip] + [_dp] * 5 + [C.c_void_p, C.POINTER(OrcParams)]
     L.orc_gravity.argtypes = [C.c_int, C.c_void_p, C.c_int] + [_dp] * 9 + [C.POINTER(OrcParams)]
+    L.orc_gravity_src.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int] + [_dp] * 9 + [C.POINTER(OrcParams)]
     L.orc_solve_range_tgt.argtypes = [C.c_int, _ip, C.c_int, _dp, _dp, _dp, _dp, _dp, _ip, _ip,
                                       C.POINTER(OrcParams)]
     L.orc_find_ngb_tgt.argtypes = [C.c_int, _ip, C.c_int, _dp, _dp, _dp, _dp, _ip, _lp, C.c_void_p]
@@ -235,6 +236,16 @@ def hydro_sample(s: dict, targets, params: OrcParams):
         "x", "y", "z", "range", "vx", "vy", "vz", "m", "rho", "P", "divv", "curlv", "omega", "psi")],
         out["ax"], out["ay"], out["az"], out["du"], out["vsig"], C.byref(params))
     return out
+
+
+def gravity_sources(x, y, z, m, rng, params: OrcParams, targets, jlo: int, jhi: int):
+    """Gravity on `targets` from the sources [jlo, jhi) only."""
+    x, y, z, m, rng = _f64(x), _f64(y), _f64(z), _f64(m), _f64(rng)
+    targets = np.ascontiguousarray(targets, np.int32)
+    g = [np.zeros(targets.size) for _ in range(4)]
+    lib().orc_gravity_src(targets.size, targets.ctypes.data_as(C.c_void_p), x.size, int(jlo), int(jhi), x, y, z, m,
+                          rng, *g, C.byref(params))
+    return g
 
 
 def morton_keys(x, y, z):

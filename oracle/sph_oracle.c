@@ -774,9 +774,10 @@ static inline void spline_g(double u, double u2, double *gacc, double *gpot) {
   }
 }
 
-void orc_gravity(int nt, const int *tgt, int n, const double *x, const double *y, const double *z,
-                 const double *m, const double *range, double *gx, double *gy, double *gz, double *phi,
-                 const orc_params *p) {
+/* the sources [jlo, jhi) on targets tgt[0..nt) (NULL: every particle) */
+static void gravity_sources(int nt, const int *tgt, int n, int jlo, int jhi, const double *x, const double *y,
+                            const double *z, const double *m, const double *range, double *gx, double *gy,
+                            double *gz, double *phi, const orc_params *p) {
   int ntot = tgt ? nt : n;
   double G = p->G;
 #pragma omp parallel for schedule(dynamic, 16)
@@ -786,7 +787,7 @@ void orc_gravity(int nt, const int *tgt, int n, const double *x, const double *y
     double xi = x[i], yi = y[i], zi = z[i];
     if (p->soft_mode == 1) {
       double e2 = p->eps * p->eps;
-      for (int j = 0; j < n; j++) {
+      for (int j = jlo; j < jhi; j++) {
         double dx = xi - x[j], dy = yi - y[j], dz = zi - z[j];
         double r2 = dx * dx + dy * dy + dz * dz + e2;
         double inv = 1.0 / sqrt(r2);
@@ -796,7 +797,7 @@ void orc_gravity(int nt, const int *tgt, int n, const double *x, const double *y
       }
     } else {
       double hi2 = range[i] * range[i];
-      for (int j = 0; j < n; j++) {
+      for (int j = jlo; j < jhi; j++) {
         double dx = xi - x[j], dy = yi - y[j], dz = zi - z[j];
         double r2 = dx * dx + dy * dy + dz * dz;
         double hj2 = range[j] * range[j];
@@ -832,6 +833,22 @@ void orc_gravity(int nt, const int *tgt, int n, const double *x, const double *y
     }
     gx[t] = G * a0; gy[t] = G * a1; gz[t] = G * a2; phi[t] = G * a3;
   }
+}
+
+void orc_gravity(int nt, const int *tgt, int n, const double *x, const double *y, const double *z,
+                 const double *m, const double *range, double *gx, double *gy, double *gz, double *phi,
+                 const orc_params *p) {
+  gravity_sources(nt, tgt, n, 0, n, x, y, z, m, range, gx, gy, gz, phi, p);
+}
+
+/* the contribution of the sources [jlo, jhi) only (a shard's share of the
+ * pairs, whose sum over the shards is orc_gravity's result) */
+void orc_gravity_src(int nt, const int *tgt, int n, int jlo, int jhi, const double *x, const double *y,
+                     const double *z, const double *m, const double *range, double *gx, double *gy, double *gz,
+                     double *phi, const orc_params *p) {
+  if (jlo < 0) jlo = 0;
+  if (jhi > n) jhi = n;
+  gravity_sources(nt, tgt, n, jlo, jhi, x, y, z, m, range, gx, gy, gz, phi, p);
 }
 
 /* ------------------------------------------------------------------ */

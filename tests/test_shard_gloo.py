@@ -7,15 +7,21 @@ Here two gloo ranks play that protocol with the FP64 oracle as the compute
 engine, over the library's own partition (cudasph_shard_range):
 
 1. each rank packs the h-solve and density results of its own particles
-   (zeros elsewhere); the sum is every particle's values, bit for bit;
+   and the library's all-gather of the ranks' own slices
+   (cudasph_b200.sharded.gather_owned) gives every rank every particle's
+   values, bit for bit;
 2. each rank runs the hydro loop over its own particles' lists only -- the
    i-side sums and the j-side pair forces those pairs add to any particle
    (sph_accelerations.cpp:106-114) -- and the sum equals the whole hydro
    pass up to the order of the FP64 additions;
-3. each rank computes gravity for its own block of targets; the sum equals
-   the whole gravity pass bit for bit;
+3. each rank computes gravity over its share of the library's own work plan
+   (cudasph_gravity_plan / cudasph_gravity_item: the one-sided blocks of the
+   diagonal tiles and the symmetric tile-pair work items, each pair's force
+   on both of its particles) for the FP64 and the mixed form's plan; the sum
+   equals the whole gravity pass to the rounding of the summation order;
 and both ranks end with identical buffers.  No GPU is used.
 """
+import ctypes as C
 import os
 import socket
 
@@ -48,6 +54,51 @@ def _csr_own(off, lst, lo, hi):
     return off2, lst2
 
 
+def _plan(n, precision, rank, world=WORLD, soft=1):
+    """cudasph_gravity_plan: [tile, block, blocks lo, hi, items lo, hi, tiles, chunk]"""
+    from cudasph_b200._capi import check, lib
+    L = lib()
+    L.cudasph_gravity_plan.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
+    out = (C.c_longlong * 8)()
+    check(L.cudasph_gravity_plan(n, precision, soft, rank, world, out), "gravity_plan")
+    return list(out)
+
+
+def _item(n, item):
+    from cudasph_b200._capi import check, lib
+    L = lib()
+    L.cudasph_gravity_item.argtypes = [C.c_int, C.c_longlong, C.c_void_p, C.c_void_p, C.c_void_p]
+    r, a, b = C.c_int(), C.c_int(), C.c_int()
+    check(L.cudasph_gravity_item(n, item, C.byref(r), C.byref(a), C.byref(b)), "gravity_item")
+    return r.value, a.value, b.value
+
+
+def _plan_gravity(ic, rng, par, n, precision, rank):
+    """This rank's gravity contributions over its share of the library's plan,
+    computed by the oracle pair by pair group: a one-sided block's particles
+    against the sources of their own tile (all sources when the tile is 0), a
+    work item's i-tile against its j-tiles and the j-tiles against the i-tile."""
+    tile, block, b0, b1, i0, i1, nt, chunk = _plan(n, precision, rank)
+    g = np.zeros((n, 4))
+    xs = (ic["x"], ic["y"], ic["z"], ic["m"], rng)
+
+    def add(tg, jlo, jhi):
+        r = O.gravity_sources(*xs, par, tg, jlo, jhi)
+        g[tg] += np.stack(r, 1)
+
+    for blk in range(b0, b1):
+        lo, hi = blk * block, min((blk + 1) * block, n)
+        jlo, jhi = ((lo // tile) * tile, min((lo // tile + 1) * tile, n)) if tile else (0, n)
+        add(np.arange(lo, hi, dtype=np.int32), jlo, jhi)
+    for it in range(i0, i1):
+        row, tlo, thi = _item(n, it)
+        ilo, ihi = row * tile, min((row + 1) * tile, n)
+        jlo, jhi = tlo * tile, min(thi * tile, n)
+        add(np.arange(ilo, ihi, dtype=np.int32), jlo, jhi)
+        add(np.arange(jlo, jhi, dtype=np.int32), ilo, ihi)
+    return g
+
+
 def _rank_main(rank, port, out_dir):
     import torch
     import torch.distributed as dist
@@ -56,7 +107,7 @@ def _rank_main(rank, port, out_dir):
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=WORLD)
     try:
-        ic = ics.polytrope(3000, n_ngb=50, seed=17)
+        ic = ics.polytrope(5000, n_ngb=50, seed=17)
         rs = np.random.default_rng(3)
         for k in ("vx", "vy", "vz"):
             ic[k] = rs.normal(0, 0.1, ic["x"].size)
@@ -70,15 +121,17 @@ def _rank_main(rank, port, out_dir):
         l0, l1 = shard_range(nleaf, rank, WORLD)
         lo, hi = l0 * KLEAF, min(l1 * KLEAF, n)
 
-        # 1. SPH exchange: own h-solve + density results, zeros elsewhere
+        # 1. SPH exchange: own h-solve + density results, gathered from their owners
+        from cudasph_b200.sharded import gather_owned, particle_spans
+        assert particle_spans(n, WORLD)[rank] == (lo, hi)
         d = O.density(s, off, lst)
         cols = [rng, d["rho"], d["divv"], d["curlv"], d["omega"], d["psi"], cnt.astype(np.float64)]
         full = np.stack(cols, 1)
-        x = np.zeros_like(full)
+        x = np.full_like(full, np.nan)  # only the own slice is valid before the exchange
         x[lo:hi] = full[lo:hi]
-        t = torch.from_numpy(x)
-        dist.all_reduce(t)
-        xsum = t.numpy()
+        t = torch.from_numpy(x.reshape(-1).copy())
+        gather_owned(t, n, rank, WORLD)
+        xsum = t.numpy().reshape(n, -1)
         s.update(rho=xsum[:, 1], divv=xsum[:, 2], curlv=xsum[:, 3], omega=xsum[:, 4], psi=xsum[:, 5])
         s["P"] = O.pressure(s["rho"], s["u"], s["mu"], par)
 
@@ -92,20 +145,19 @@ def _rank_main(rank, port, out_dir):
             hs[k] = t.numpy()
         href = O.hydro(s, off, lst, par)
 
-        # 3. gravity: own block of targets (the one-sided decomposition)
-        nb = (n + 255) // 256
-        b0, b1 = shard_range(nb, rank, WORLD)
-        tg = np.arange(b0 * 256, min(b1 * 256, n), dtype=np.int32)
-        g = O.gravity(ic["x"], ic["y"], ic["z"], ic["m"], rng, par, targets=tg)
-        gbuf = np.zeros((n, 4))
-        gbuf[tg] = np.stack(g, 1)
-        t = torch.from_numpy(gbuf)
-        dist.all_reduce(t)
-        gsum = t.numpy()
-        gref = np.stack(O.gravity(ic["x"], ic["y"], ic["z"], ic["m"], rng, par), 1)
+        # 3. gravity over this rank's share of the library's work plan (Plummer)
+        gpar = O.make_params(n_target=50.0, eos_mode=1, soft_mode=1, eps=0.01)
+        gref = np.stack(O.gravity(ic["x"], ic["y"], ic["z"], ic["m"], rng, gpar), 1)
+        gsums, plans = [], []
+        for prec in (0, 1):
+            gbuf = _plan_gravity(ic, rng, gpar, n, prec, rank)
+            t = torch.from_numpy(gbuf)
+            dist.all_reduce(t)
+            gsums.append(t.numpy())
+            plans.append(_plan(n, prec, rank))
 
-        np.savez(os.path.join(out_dir, f"rank{rank}.npz"), xsum=xsum, full=full, gsum=gsum, gref=gref,
-                 own=np.array([lo, hi]), **{"h_" + k: v for k, v in hs.items()},
+        np.savez(os.path.join(out_dir, f"rank{rank}.npz"), xsum=xsum, full=full, gsum0=gsums[0], gsum1=gsums[1],
+                 gref=gref, own=np.array([lo, hi]), plans=np.array(plans), **{"h_" + k: v for k, v in hs.items()},
                  **{"r_" + k: href[k] for k in hs})
     finally:
         dist.destroy_process_group()
@@ -120,11 +172,16 @@ def test_sharded_exchanges_on_two_gloo_ranks(tmp_path):
     assert r[0]["own"][0] == 0 and r[0]["own"][1] == r[1]["own"][0] and r[1]["own"][1] == r[0]["full"].shape[0]
     assert r[0]["own"][1] > 0 and r[1]["own"][1] > r[1]["own"][0]
     for k in r[0].files:  # identical state on both ranks
-        if k != "own":
+        if k not in ("own", "plans"):
             assert np.array_equal(r[0][k], r[1][k]), k
     a = r[0]
     assert np.array_equal(a["xsum"], a["full"])
-    assert np.array_equal(a["gsum"], a["gref"])
+    # both plans split the work between the ranks (one-sided blocks and items)
+    p0, p1 = r[0]["plans"], r[1]["plans"]
+    for q in range(2):
+        assert p0[q][3] == p1[q][2] and p0[q][5] == p1[q][4] and p0[q][5] > p0[q][4] >= 0
+    for k in ("gsum0", "gsum1"):
+        assert np.max(np.abs(a[k] - a["gref"]), axis=0).max() <= 1e-13 * np.abs(a["gref"]).max(), k
     for k in ("ax", "ay", "az", "du"):
         ref = a["r_" + k]
         assert np.max(np.abs(a["h_" + k] - ref)) <= 1e-12 * np.max(np.abs(ref)), k
@@ -141,3 +198,32 @@ def test_shard_range_partitions(count, world):
         assert a1 == b0
     sizes = [h - l for l, h in spans]
     assert min(sizes) >= 0 and max(sizes) - min(sizes) <= 1
+
+
+@pytest.mark.parametrize("n", [1, 1000, 3000, 20001, 70000, 1 << 20])
+@pytest.mark.parametrize("world", [1, 2, 3, 8])
+@pytest.mark.parametrize("precision,soft", [(0, 1), (1, 1), (0, 0), (1, 0)])
+def test_gravity_plan_covers_every_pair_once(n, world, precision, soft):
+    """The library's gravity work plan, without a device: the ranks' one-sided
+    blocks partition the blocks of all n particles, their symmetric items
+    partition the items, each item's j-tiles lie above its i-tile, and the
+    items cover every pair of distinct tiles exactly once (the diagonal tiles
+    are the one-sided blocks' own-tile pairs)."""
+    plans = [_plan(n, precision, r, world, soft) for r in range(world)]
+    tile, block, _, _, _, _, nt, chunk = plans[0]
+    assert all(p[0] == tile and p[1] == block and p[6] == nt and p[7] == chunk for p in plans)
+    nblocks = (n + block - 1) // block
+    assert plans[0][2] == 0 and plans[-1][3] == nblocks
+    assert all(a[3] == b[2] for a, b in zip(plans, plans[1:]))
+    if soft == 0 or nt < 2:
+        assert tile == 0 and all(p[4] == p[5] for p in plans)
+        return
+    assert tile % block == 0
+    assert plans[0][4] == 0 and all(a[5] == b[4] for a, b in zip(plans, plans[1:]))
+    seen = np.zeros((nt, nt), np.int32)
+    for it in range(plans[-1][5]):
+        row, tlo, thi = _item(n, it)
+        assert row < tlo < thi <= nt and thi - tlo <= chunk
+        seen[row, tlo:thi] += 1
+    upper = np.triu(np.ones((nt, nt), np.int32), 1)
+    assert np.array_equal(seen, upper)
