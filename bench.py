@@ -20,17 +20,28 @@ larger than L2, so no flush is needed between steps.
   e2e          the same through the C ABI with host buffers: every step copies
                the state in from pinned host memory and the result out
   fp64         the plain FP64 step on the same workload, and the mixed/fp64
-               ratio; errors = mixed vs FP64 accelerations at the same state
+               ratio; errors = mixed vs FP64 accelerations at the same state,
+               and (errors.against_oracle) every GPU form vs the FP64 oracle
   roofline     the direct-N gravity kernel on the FP32 FMA pipe: 20 flops per
                pair interaction x N^2 per launch / launch time, against the
                FP32 FMA peak measured in the same run
-  cpu_baseline the reference's own code built for the host CPU (oracle/_ref),
-               on a bounded sample (see 'sample')
+  adjoint      reverse sweep / forward step at the h solve's forward default
+               and at the gradient tests' tolerance
+  drift_100    energy drift over 100 steps, mixed and FP64 side by side
+  dropin       the reference's own driver on this library (N = 262,144)
+  large_c5     the N = 4,194,304 cold-sphere workload (5 mixed steps, tree
+               gravity, a subset adjoint)
+  cpu_baseline the FP64 oracle at this workload's own parameters on a bounded
+               sample (see 'sample'; measured and extrapolated seconds are
+               labelled), with the reference's own CPU build beside it
+  c2_per_kernel the N = 262,144 FP64 workload, each kernel against its CPU
+               counterparts
 
---impl reference times only the reference's CPU build on the same workload.
-Under torchrun (N > 1) the ranks share ONE simulation of the same workload
-(cudasph_b200.sharded: SPH leaf ranges and gravity work items per rank, three
-NCCL all-reduces per step; strong scaling); rank 0 prints.
+--impl reference times the reference's CPU build on the same workload (and
+the oracle at the workload's parameters once).  Under torchrun (N > 1) the
+ranks share ONE simulation of the same workload (cudasph_b200.sharded: SPH
+leaf ranges and gravity work items per rank, an all-gather and two
+all-reduces per step; strong scaling); rank 0 prints.
 """
 from __future__ import annotations
 
@@ -866,6 +877,10 @@ def run_ours(args, rank, world):
         if "s_per_step" in di:
             out["dropin_s_per_step"] = di["s_per_step"]
 
+    # --- the other named workloads: C5 (N = 4M cold sphere, gravity-dominated) ---------
+    if args.large_line:
+        out["large_c5"] = large_run()
+
     # --- CPU baseline: the FP64 oracle at this workload's own parameters (and the ------
     # --- checker of the first steps above), the reference's own code beside it ---------
     if args.cpu_baseline:
@@ -889,6 +904,11 @@ def run_ours(args, rank, world):
         out["cpu_baseline"] = cb
         if against and "errors" in out:
             out["errors"]["against_oracle"] = against
+        # C2 (N = 262,144, plain FP64): each kernel on the GPU against its CPU
+        # counterparts (the oracle at the workload's parameters, the
+        # reference's own build at its compiled-in ones)
+        if args.c2_line:
+            out["c2_per_kernel"] = c2_run()
     return out
 
 
@@ -1069,6 +1089,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--drift-line-steps", type=int, default=100,
                     help="energy drift over this many steps of the mixed and FP64 forms in the bench line (0: skip)")
+    ap.add_argument("--no-large-line", dest="large_line", action="store_false",
+                    help="skip the N = 4,194,304 cold-sphere run (C5) in the bench line")
+    ap.add_argument("--no-c2-line", dest="c2_line", action="store_false",
+                    help="skip the N = 262,144 per-kernel GPU / CPU table (C2) in the bench line")
     ap.add_argument("--dropin-steps", type=int, default=3,
                     help="steps of the reference's own driver on this library (N = 262,144; 0: skip)")
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false")
