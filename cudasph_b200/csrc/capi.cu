@@ -24,7 +24,9 @@ int peano_keys(int n, const double4 *pos, const double *x, const double *y, cons
 int tree_layout(int n, TreeView *t);
 int build_tree(const TreeView &t, const double4 *pos, float4 *lo, float4 *hi, cudaStream_t st);
 int launch_solve_range(const TreeView &t, double4 *pos, int *nevals, unsigned *flags, const sph_params &p,
-                       int *n_ngb, int *list, double *dcache, int cap, int leaf0, int leaf1, cudaStream_t st);
+                       int *n_ngb, int *list, double *dcache, int cap, void *work, int leaf0, int leaf1,
+                       cudaStream_t st);
+size_t solve_work_bytes(int n, int nleaf);
 int launch_find_ngb(const TreeView &t, const double4 *pos, int *n_ngb, int *list, int cap, unsigned *flags,
                     int leaf0, int leaf1, cudaStream_t st);
 int launch_density(const HydroArgs &a, cudaStream_t st);
@@ -87,6 +89,7 @@ struct sph_ctx {
   int *n_ngb = nullptr, *nevals = nullptr, *list = nullptr;
   int list_cap = 0;  // per particle
   double *dcache = nullptr;  // candidate squared distances of the h solve, layout of list
+  char *solve_work = nullptr;  // queue and saved lane states between the h solve's two kernels
   TreeView tree;
   float4 *tlo = nullptr, *thi = nullptr;
   void *tgws = nullptr;  // tree-gravity workspace (radix tree + node moments)
@@ -297,7 +300,7 @@ extern "C" int cudasph_destroy(sph_ctx *c) {
   }
   cudaFree(c->old); cudaFree(c->n_ngb); cudaFree(c->nevals); cudaFree(c->list); cudaFree(c->dcache);
   cudaFree(c->tlo); cudaFree(c->thi); cudaFree(c->tgws); cudaFree(c->keys); cudaFree(c->vals); cudaFree(c->sort_scratch);
-  cudaFree(c->bbox_part); cudaFree(c->box4); cudaFree(c->aux); cudaFree(c->gsrc); cudaFree(c->gh2); cudaFree(c->mass_mixed); cudaFree(c->xbuf); cudaFree(c->flags);
+  cudaFree(c->bbox_part); cudaFree(c->box4); cudaFree(c->aux); cudaFree(c->solve_work); cudaFree(c->gsrc); cudaFree(c->gh2); cudaFree(c->mass_mixed); cudaFree(c->xbuf); cudaFree(c->flags);
   cudaFree(c->sc); cudaFree(c->fin_part); cudaFree(c->flat); cudaFree(c->slot_of);
   cudaFree(c->pre_acc); cudaFree(c->dsum); cudaFree(c->xb); cudaFree(c->vb); cudaFree(c->ab); cudaFree(c->vpb); cudaFree(c->vpup);
   cudaFree(c->rhob); cudaFree(c->Pb); cudaFree(c->omb); cudaFree(c->psib); cudaFree(c->divb); cudaFree(c->curlb);
@@ -358,6 +361,7 @@ extern "C" int cudasph_create(const sph_params *params, int n, int device, sph_c
   TRY_ALLOC(dalloc(&c->bbox_part, 148 * 2 * 6));
   TRY_ALLOC(dalloc(&c->box4, 4));
   TRY_ALLOC(dalloc(&c->aux, n));
+  TRY_ALLOC(dalloc(&c->solve_work, solve_work_bytes(n, c->tree.count[0])));
   TRY_ALLOC(dalloc(&c->gsrc, n));
   TRY_ALLOC(dalloc(&c->gh2, n));
   TRY_ALLOC(dalloc(&c->mass_mixed, 1));
@@ -632,7 +636,7 @@ extern "C" int cudasph_solve_range(sph_ctx *c) {
   int leaf0, leaf1;
   shard_leaves(c, leaf0, leaf1);
   LAUNCHED(launch_solve_range(c->tree, c->f[c->cur].pos, c->nevals, c->flags, c->p, c->n_ngb, c->list, c->dcache,
-                              c->list_cap, leaf0, leaf1, c->st));
+                              c->list_cap, c->solve_work, leaf0, leaf1, c->st));
   // the solve writes the neighbour lists at the final ranges (find_ngb fused)
   c->lists_ok = true;
   c->density_ok = false;

@@ -243,7 +243,11 @@ struct SolveArgs {
   double *dcache;  // squared distances of the cached candidates, layout of list
   int cap;
   int leaf0, leaf1;  // leaves processed by this launch
-  int speculate;     // first evaluation by a walk at the range itself (see k_solve_range)
+  // the speculative first pass (k_solve_spec) hands the leaves it leaves
+  // unfinished to k_solve_range through a queue (null: no speculative pass)
+  int *queue;
+  int *queue_count;
+  struct SolveSave *save;  // per slot
 };
 
 enum { kBr0 = 0, kBr1 = 1, kSolve = 2, kDone = 3 };
@@ -252,7 +256,84 @@ enum { kBr0 = 0, kBr1 = 1, kSolve = 2, kDone = 3 };
 // clamped Newton step of the bracket (f_scale = 10 %) stays inside it
 constexpr double kCacheMargin = 1.15;
 constexpr int kEvalBatch = 4;     // cache entries loaded ahead per evaluation step
+constexpr int kSpecBlocks = 8;    // resident blocks per SM of the speculative pass
 constexpr int kCompactBatch = 8;  // cache entries loaded ahead per compaction step
+
+// A lane's iteration state: the bracket / Newton / bisection steps of
+// dev_solve_range.cu:93-172 between evaluations.
+struct LaneIter {
+  double w, dx, f, x_left, f_try, rx, ry;
+  int phase, iter, keep, nev;
+};
+
+// One evaluation's epilogue (compute_ngb, dev_solve_range.cu:77-87) with the
+// smooth count sf and its derivative sum sg at it.w, and the step of the
+// lane's iteration to its next evaluation or the end.
+__device__ __forceinline__ void solve_advance(LaneIter &it, double sf, double sg, const SolveArgs &a) {
+  const double rel = a.rel_err, fs = a.f_scale;
+    it.nev++;
+  it.f = sf - a.n_target;
+  sg *= 1.0 / it.w;
+  if (sg != 0) it.dx = it.f / sg;
+  else it.dx = (it.f < 0) ? -it.w : +it.w;
+  bool to_solve_init = false, to_br_check = false, to_solve_check = false;
+  if (it.phase == kBr0 || it.phase == kBr1) {
+    if (fabs(it.dx) < rel * it.w) {
+      it.rx = it.w - 0.5 * fabs(it.dx);
+      it.ry = it.w + 0.5 * fabs(it.dx);
+      to_solve_init = true;
+    } else {
+      if (fabs(it.dx) > fs * it.w) it.dx = (it.dx < 0) ? -fs * it.w : fs * it.w;
+      if (it.phase == kBr0) {
+        it.x_left = it.w;
+        it.f_try = it.f;
+        it.iter = 0;
+      }
+      to_br_check = true;
+    }
+  } else {  // kSolve
+    if (it.f < 0) it.rx = it.w;
+    else it.ry = it.w;
+    it.keep = fabs(it.dx) > rel * it.w;
+    to_solve_check = true;
+  }
+  if (to_br_check) {
+    if ((it.f_try * it.f >= 0) && (it.iter++ < a.max_iter)) {
+      it.x_left = it.w;
+      it.f_try = it.f;
+      it.w -= it.dx;
+      it.phase = kBr1;
+    } else {
+      if (it.x_left < it.w) { it.rx = it.x_left; it.ry = it.w; }
+      else { it.rx = it.w; it.ry = it.x_left; }
+      to_solve_init = true;
+    }
+  }
+  if (to_solve_init) {
+    it.w = 0.5 * (it.rx + it.ry);
+    it.dx = 0;
+    if (fabs(it.rx - it.ry) > rel * it.w) {
+      it.iter = 0;
+      it.keep = 1;
+      to_solve_check = true;
+    } else {
+      it.phase = kDone;
+    }
+  }
+  if (to_solve_check) {
+    if (it.keep && (it.iter++ < a.max_iter)) {
+      it.w -= it.dx;
+      if ((it.w - it.ry) * (it.w - it.rx) >= 0) {
+        it.dx = 0.5 * (it.ry - it.rx);
+        it.w = 0.5 * (it.rx + it.ry);
+      }
+      it.phase = kSolve;
+    } else {
+      if (it.keep) raise_flag(a.flags, SPH_FLAG_H_NOT_CONVERGED);
+      it.phase = kDone;
+    }
+  }
+}
 
 // dev_solve_range (dev_solve_range.cu:137-189): per particle, bracket the
 // root of f(w) = sum_j ig(2 r_ij / w) - N_target with clamped Newton steps
@@ -272,123 +353,66 @@ constexpr int kCompactBatch = 8;  // cache entries loaded ahead per compaction s
 // when the final range differs from the last one evaluated (`pending`).
 // 6 blocks (24 warps) per SM: at N = 1M the capped form (80 registers, a
 // few spilled) took 12.1 ms per solve against 14.5 ms at 120 registers.
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, 6) k_solve_range(SolveArgs a) {
+// a lane's state handed from the speculative pass to the resumed solve
+struct SolveSave {
+  double w, dx, f, x_left, f_try, rx, ry;
+  int phase, iter, keep, nev, cnt_list, bits;  // bits: 1 direct, 2 pending, 4 listed by the speculative pass
+};
+
+// Speculative first evaluation.  In steady state the previous step's range
+// (after the predictor) already passes the tolerance test for almost every
+// particle, so the first evaluation is also the last: the warp walks the
+// tree once at the ranges themselves, every hit (d2 < w^2) goes straight to
+// its lane's list (index only), and each lane evaluates f and f' over its
+// list in list order -- ascending index, the order of the walk and of the
+// CPU loop -- recomputing the FP64 d2 of each entry from the positions (the
+// same operations as the walk, so the same value).  No candidate cache is
+// written or read.  A lane done after this evaluation keeps the list when
+// its final range (w = (rx + ry) / 2, within a few ulp of the evaluated one)
+// leaves the set unchanged: every entry inside the final range (the largest
+// d2 checked), and, if the range grew, no candidate in the sliver just
+// outside the evaluated range (flagged during the walk).  Otherwise the
+// lane lists by a walk at its final range; lanes not done continue with the
+// candidate cache below.
+// This is its own kernel, with fewer registers (more resident warps) than
+// the candidate-cache solve; a leaf with a lane not done after it saves its
+// lanes' states and goes on a queue that k_solve_range then resumes.
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, kSpecBlocks) k_solve_spec(SolveArgs a) {
   __shared__ WarpSmem smem[kWarpsPerBlock];
   WarpSmem &sm = smem[threadIdx.x >> 5];
   const int leaf = a.leaf0 + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  const int n = a.t.n;
   if (leaf >= a.leaf1) return;
+  const int n = a.t.n;
   const int s = leaf * kLeaf + (int)lane_id();
   const bool valid = s < n;
-  double xi = 0, yi = 0, zi = 0, w = 0;
+  double xi = 0, yi = 0, zi = 0, w0 = 0;
   if (valid) {
     const double4 p = a.pos[s];
-    xi = p.x; yi = p.y; zi = p.z; w = p.w;
+    xi = p.x; yi = p.y; zi = p.z; w0 = p.w;
   }
-  const Prefilter pf = make_prefilter(valid && w > 0, xi, yi, zi);
+  const Prefilter pf = make_prefilter(valid && w0 > 0, xi, yi, zi);
   sm.tx[lane_id()] = xi;
   sm.ty[lane_id()] = yi;
   sm.tz[lane_id()] = zi;
   __syncwarp();
   const size_t colbase = (size_t)leaf * a.cap * kLeaf;  // the warp's block of list / dcache
-  int phase = (valid && w > 0) ? kBr0 : kDone;
-  double dx = 0, f = 0, x_left = 0, f_try = 0, rx = 0, ry = 0;
-  int iter = 0, keep = 0, nev = 0;
+  LaneIter it;
+  it.w = w0;
+  it.phase = (valid && w0 > 0) ? kBr0 : kDone;
+  it.dx = it.f = it.x_left = it.f_try = it.rx = it.ry = 0;
+  it.iter = it.keep = it.nev = 0;
+  double &w = it.w;
+  int &phase = it.phase, &nev = it.nev;
   bool stack_ok = true;
-  const double rel = a.rel_err, fs = a.f_scale;
   const size_t col = (size_t)leaf * a.cap * kLeaf + lane_id();
   int *lst = a.list + col;
-  double *dc = a.dcache + col;
   const int cap = a.cap;
-  int ncache = 0;           // cached entries
-  double cache_r2 = -1.0;   // the cache holds every j with d2 < cache_r2
-  bool direct = false;
-  double w_list = -1.0;     // direct lanes: range of the list last written
   int cnt_list = 0;
+  bool direct = false;
   bool pending = false;
-  // One evaluation's epilogue (compute_ngb, dev_solve_range.cu:77-87) and
-  // the step of the lane's iteration to its next evaluation or the end.
-  auto advance = [&](double sf, double sg) {
-    nev++;
-    f = sf - a.n_target;
-    sg *= 1.0 / w;
-    if (sg != 0) dx = f / sg;
-    else dx = (f < 0) ? -w : +w;
-    bool to_solve_init = false, to_br_check = false, to_solve_check = false;
-    if (phase == kBr0 || phase == kBr1) {
-      if (fabs(dx) < rel * w) {
-        rx = w - 0.5 * fabs(dx);
-        ry = w + 0.5 * fabs(dx);
-        to_solve_init = true;
-      } else {
-        if (fabs(dx) > fs * w) dx = (dx < 0) ? -fs * w : fs * w;
-        if (phase == kBr0) {
-          x_left = w;
-          f_try = f;
-          iter = 0;
-        }
-        to_br_check = true;
-      }
-    } else {  // kSolve
-      if (f < 0) rx = w;
-      else ry = w;
-      keep = fabs(dx) > rel * w;
-      to_solve_check = true;
-    }
-    if (to_br_check) {
-      if ((f_try * f >= 0) && (iter++ < a.max_iter)) {
-        x_left = w;
-        f_try = f;
-        w -= dx;
-        phase = kBr1;
-      } else {
-        if (x_left < w) { rx = x_left; ry = w; }
-        else { rx = w; ry = x_left; }
-        to_solve_init = true;
-      }
-    }
-    if (to_solve_init) {
-      w = 0.5 * (rx + ry);
-      dx = 0;
-      if (fabs(rx - ry) > rel * w) {
-        iter = 0;
-        keep = 1;
-        to_solve_check = true;
-      } else {
-        phase = kDone;
-      }
-    }
-    if (to_solve_check) {
-      if (keep && (iter++ < a.max_iter)) {
-        w -= dx;
-        if ((w - ry) * (w - rx) >= 0) {
-          dx = 0.5 * (ry - rx);
-          w = 0.5 * (rx + ry);
-        }
-        phase = kSolve;
-      } else {
-        if (keep) raise_flag(a.flags, SPH_FLAG_H_NOT_CONVERGED);
-        phase = kDone;
-      }
-    }
-  };
-  // Speculative first evaluation.  In steady state the previous step's range
-  // (after the predictor) already passes the tolerance test for almost every
-  // particle, so the first evaluation is also the last: the warp walks the
-  // tree once at the ranges themselves, every hit (d2 < w^2) goes straight to
-  // its lane's list (index only), and each lane evaluates f and f' over its
-  // list in list order -- ascending index, the order of the walk and of the
-  // CPU loop -- recomputing the FP64 d2 of each entry from the positions (the
-  // same operations as the walk, so the same value).  No candidate cache is
-  // written or read.  A lane done after this evaluation keeps the list when
-  // its final range (w = (rx + ry) / 2, within a few ulp of the evaluated one)
-  // leaves the set unchanged: every entry inside the final range (the largest
-  // d2 checked), and, if the range grew, no candidate in the sliver just
-  // outside the evaluated range (flagged during the walk).  Otherwise the
-  // lane lists by a walk at its final range; lanes not done continue with the
-  // candidate cache below.
+  auto advance = [&](double sf, double sg) { solve_advance(it, sf, sg, a); };
   int spec_cnt = -1;  // >= 0: the speculative list is this lane's final list
-  if (a.speculate && __any_sync(kFull, phase != kDone)) {
+  if (__any_sync(kFull, phase != kDone)) {
     const bool on = phase != kDone;
     const double w_eval = w;
     const double r2 = __dmul_rn(w, w);
@@ -472,6 +496,75 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 6) k_solve_range(SolveArg
         }
       }
     }
+  }
+  if (!stack_ok && lane_id() == 0) raise_flag(a.flags, SPH_FLAG_STACK_OVERFLOW);
+  const bool more = phase != kDone || pending;
+  if (!__any_sync(kFull, more)) {
+    if (valid) {
+      a.pos[s].w = (w > 0) ? w : 0.0;
+      a.n_ngb[s] = cnt_list;
+      if (a.nevals) a.nevals[s] = nev;
+    }
+    return;
+  }
+  if (valid) {
+    SolveSave v;
+    v.w = it.w; v.dx = it.dx; v.f = it.f; v.x_left = it.x_left; v.f_try = it.f_try; v.rx = it.rx; v.ry = it.ry;
+    v.phase = it.phase; v.iter = it.iter; v.keep = it.keep; v.nev = it.nev; v.cnt_list = cnt_list;
+    v.bits = (direct ? 1 : 0) | (pending ? 2 : 0) | (spec_cnt >= 0 ? 4 : 0);
+    a.save[s] = v;
+  }
+  if (lane_id() == 0) a.queue[atomicAdd(a.queue_count, 1)] = leaf;
+}
+
+// The candidate-cache solve of one leaf-warp, from the initial ranges or
+// (resume) from the states the speculative pass saved.
+__device__ __forceinline__ void solve_leaf(const SolveArgs &a, WarpSmem &sm, int leaf, bool resume) {
+  const int n = a.t.n;
+  const int s = leaf * kLeaf + (int)lane_id();
+  const bool valid = s < n;
+  double xi = 0, yi = 0, zi = 0, w0 = 0;
+  if (valid) {
+    const double4 p = a.pos[s];
+    xi = p.x; yi = p.y; zi = p.z; w0 = p.w;
+  }
+  const Prefilter pf = make_prefilter(valid && w0 > 0, xi, yi, zi);
+  sm.tx[lane_id()] = xi;
+  sm.ty[lane_id()] = yi;
+  sm.tz[lane_id()] = zi;
+  __syncwarp();
+  const size_t colbase = (size_t)leaf * a.cap * kLeaf;  // the warp's block of list / dcache
+  LaneIter it;
+  it.w = w0;
+  it.phase = (valid && w0 > 0) ? kBr0 : kDone;
+  it.dx = it.f = it.x_left = it.f_try = it.rx = it.ry = 0;
+  it.iter = it.keep = it.nev = 0;
+  double &w = it.w;
+  int &phase = it.phase, &nev = it.nev;
+  bool stack_ok = true;
+  const size_t col = (size_t)leaf * a.cap * kLeaf + lane_id();
+  int *lst = a.list + col;
+  const int cap = a.cap;
+  int cnt_list = 0;
+  bool direct = false;
+  bool pending = false;
+  auto advance = [&](double sf, double sg) { solve_advance(it, sf, sg, a); };
+  double &dx = it.dx, &f = it.f, &x_left = it.x_left, &f_try = it.f_try, &rx = it.rx, &ry = it.ry;
+  int &iter = it.iter, &keep = it.keep;
+  (void)dx; (void)f; (void)x_left; (void)f_try; (void)rx; (void)ry; (void)iter; (void)keep;
+  double *dc = a.dcache + col;
+  int ncache = 0;           // cached entries
+  double cache_r2 = -1.0;   // the cache holds every j with d2 < cache_r2
+  double w_list = -1.0;     // direct lanes: range of the list last written
+  int spec_cnt = -1;        // >= 0: the speculative pass listed this lane
+  if (resume && valid) {
+    const SolveSave v = a.save[s];
+    it.w = v.w; it.dx = v.dx; it.f = v.f; it.x_left = v.x_left; it.f_try = v.f_try; it.rx = v.rx; it.ry = v.ry;
+    it.phase = v.phase; it.iter = v.iter; it.keep = v.keep; it.nev = v.nev;
+    cnt_list = v.cnt_list;
+    direct = (v.bits & 1) != 0;
+    pending = (v.bits & 2) != 0;
+    spec_cnt = (v.bits & 4) ? v.cnt_list : -1;
   }
   while (true) {
     const bool iterate = phase != kDone;
@@ -645,6 +738,24 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 6) k_solve_range(SolveArg
   }
 }
 
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, 6) k_solve_range(SolveArgs a) {
+  __shared__ WarpSmem smem[kWarpsPerBlock];
+  WarpSmem &sm = smem[threadIdx.x >> 5];
+  const int wid = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (!a.queue) {
+    const int leaf = a.leaf0 + wid;
+    if (leaf < a.leaf1) solve_leaf(a, sm, leaf, false);
+    return;
+  }
+  // the leaves the speculative pass left, handed out to the resident warps
+  const int nw = (int)((gridDim.x * blockDim.x) >> 5);
+  const int count = *a.queue_count;
+  for (int q = wid; q < count; q += nw) {
+    solve_leaf(a, sm, a.queue[q], true);
+    __syncwarp();
+  }
+}
+
 struct FindArgs {
   TreeView t;
   const double4 *pos;
@@ -706,21 +817,40 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_find_ngb(FindArgs a) {
   if (valid) a.n_ngb[s] = cnt;
 }
 
+// scratch of the two-kernel solve: the queue count, the queue, the saved states
+size_t solve_work_bytes(int n, int nleaf) {
+  return 256 + ((size_t)nleaf * sizeof(int) + 255) / 256 * 256 + (size_t)n * sizeof(SolveSave);
+}
+
 // leaves [leaf0, leaf1) (a shard's range, or 0 and the leaf count)
 int launch_solve_range(const TreeView &t, double4 *pos, int *nevals, unsigned *flags, const sph_params &p,
-                       int *n_ngb, int *list, double *dcache, int cap, int leaf0, int leaf1, cudaStream_t st) {
+                       int *n_ngb, int *list, double *dcache, int cap, void *work, int leaf0, int leaf1,
+                       cudaStream_t st) {
   SolveArgs a;
   a.t = t; a.pos = pos; a.nevals = nevals; a.flags = flags;
   a.n_ngb = n_ngb; a.list = list; a.dcache = dcache; a.cap = cap;
   a.n_target = p.n_target; a.rel_err = p.rel_err; a.f_scale = p.f_scale; a.max_iter = p.max_iter;
   a.leaf0 = leaf0; a.leaf1 = leaf1;
-  // the speculative first evaluation pays when the previous range is likely
-  // to pass the tolerance test already (not with a tight tolerance)
-  a.speculate = p.rel_err >= 1e-8;
+  a.queue = nullptr; a.queue_count = nullptr; a.save = nullptr;
   const int warps = leaf1 - leaf0;
   if (warps <= 0) return 0;
-  k_solve_range<<<(warps + kWarpsPerBlock - 1) / kWarpsPerBlock, kWarpsPerBlock * 32, 0, st>>>(a);
-  return 1;
+  const int blocks = (warps + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  // the speculative first evaluation pays when the previous range is likely
+  // to pass the tolerance test already (not with a tight tolerance)
+  if (p.rel_err < 1e-8 || !work) {
+    k_solve_range<<<blocks, kWarpsPerBlock * 32, 0, st>>>(a);
+    return 1;
+  }
+  char *w = (char *)work;
+  a.queue_count = (int *)w;
+  a.queue = (int *)(w + 256);
+  a.save = (SolveSave *)(w + 256 + ((size_t)t.count[0] * sizeof(int) + 255) / 256 * 256);
+  cudaMemsetAsync(a.queue_count, 0, sizeof(int), st);
+  k_solve_spec<<<blocks, kWarpsPerBlock * 32, 0, st>>>(a);
+  // the resumed leaves (about a tenth in steady state) on the resident warps
+  const int resident = 148 * 6;
+  k_solve_range<<<blocks < resident ? blocks : resident, kWarpsPerBlock * 32, 0, st>>>(a);
+  return 2;
 }
 
 int launch_find_ngb(const TreeView &t, const double4 *pos, int *n_ngb, int *list, int cap, unsigned *flags,
