@@ -271,7 +271,7 @@ struct LaneIter {
 // lane's iteration to its next evaluation or the end.
 __device__ __forceinline__ void solve_advance(LaneIter &it, double sf, double sg, const SolveArgs &a) {
   const double rel = a.rel_err, fs = a.f_scale;
-    it.nev++;
+  it.nev++;
   it.f = sf - a.n_target;
   sg *= 1.0 / it.w;
   if (sg != 0) it.dx = it.f / sg;
@@ -335,24 +335,6 @@ __device__ __forceinline__ void solve_advance(LaneIter &it, double sf, double sg
   }
 }
 
-// dev_solve_range (dev_solve_range.cu:137-189): per particle, bracket the
-// root of f(w) = sum_j ig(2 r_ij / w) - N_target with clamped Newton steps
-// (dev_bracket_root :93-135), then safeguarded Newton / bisection until
-// |dx| < rel_err * w.  Each lane runs that iteration as a state machine.
-//
-// Candidate cache (find_ngb fused in): a lane whose range w is not covered
-// by its cache walks the tree once at radius 1.15 w and stores every j with
-// d2 < (1.15 w)^2 -- index in its column of the neighbour list, exact FP64
-// d2 in the same column of dcache -- in the walk's ascending order.  Every
-// evaluation of f (and of its derivative) then runs over the cached entries
-// with d2 < w^2 in that order, the same operations in the same order as a
-// walk at w, and the final list is the cache compacted in place to the final
-// range.  The lanes that need a walk in a round share it.  A lane whose
-// candidates exceed the list capacity falls back to walking at w for every
-// evaluation, writing its list as it goes (`direct`), with one list-only walk
-// when the final range differs from the last one evaluated (`pending`).
-// 6 blocks (24 warps) per SM: at N = 1M the capped form (80 registers, a
-// few spilled) took 12.1 ms per solve against 14.5 ms at 120 registers.
 // a lane's state handed from the speculative pass to the resumed solve
 struct SolveSave {
   double w, dx, f, x_left, f_try, rx, ry;
@@ -437,7 +419,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kSpecBlocks) k_solve_spec
       const int jk = lj * kLeaf + (int)lane_id();
       const unsigned below = (1u << lane_id()) - 1u;
       unsigned m = tm;
-      while (m) {  // two targets per round, as in the cache fill below
+      while (m) {  // two targets per round, as in the candidate-cache fill of k_solve_range
         const int t0 = __ffs(m) - 1;
         m &= m - 1u;
         const int t1 = m ? __ffs(m) - 1 : t0;
@@ -517,6 +499,24 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kSpecBlocks) k_solve_spec
   if (lane_id() == 0) a.queue[atomicAdd(a.queue_count, 1)] = leaf;
 }
 
+// dev_solve_range (dev_solve_range.cu:137-189): per particle, bracket the
+// root of f(w) = sum_j ig(2 r_ij / w) - N_target with clamped Newton steps
+// (dev_bracket_root :93-135), then safeguarded Newton / bisection until
+// |dx| < rel_err * w.  Each lane runs that iteration as a state machine.
+//
+// Candidate cache (find_ngb fused in): a lane whose range w is not covered
+// by its cache walks the tree once at radius 1.15 w and stores every j with
+// d2 < (1.15 w)^2 -- index in its column of the neighbour list, exact FP64
+// d2 in the same column of dcache -- in the walk's ascending order.  Every
+// evaluation of f (and of its derivative) then runs over the cached entries
+// with d2 < w^2 in that order, the same operations in the same order as a
+// walk at w, and the final list is the cache compacted in place to the final
+// range.  The lanes that need a walk in a round share it.  A lane whose
+// candidates exceed the list capacity falls back to walking at w for every
+// evaluation, writing its list as it goes (`direct`), with one list-only walk
+// when the final range differs from the last one evaluated (`pending`).
+// 6 blocks (24 warps) per SM: at N = 1M the capped form (80 registers, a
+// few spilled) took 12.1 ms per solve against 14.5 ms at 120 registers.
 // The candidate-cache solve of one leaf-warp, from the initial ranges or
 // (resume) from the states the speculative pass saved.
 __device__ __forceinline__ void solve_leaf(const SolveArgs &a, WarpSmem &sm, int leaf, bool resume) {
