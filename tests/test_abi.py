@@ -154,3 +154,28 @@ def test_noalloc_sort_validates_arguments_before_any_device_work():
     assert f(2, None, 0x20, None) == 2
     assert b"null" in L.cudasph_last_error()
     assert f(2, 0x10, None, None) == 2
+
+
+def test_gravity_plan_validates_arguments_without_a_device():
+    """cudasph_gravity_plan / cudasph_gravity_item reject bad sizes, ranks,
+    precisions, softening modes, items and null outputs with SPH_ERR_ARG,
+    and answer valid queries, all without a device."""
+    L = _capi.lib()
+    L.cudasph_gravity_plan.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
+    L.cudasph_gravity_item.argtypes = [C.c_int, C.c_longlong, C.c_void_p, C.c_void_p, C.c_void_p]
+    out = (C.c_longlong * 8)()
+    assert L.cudasph_gravity_plan(-1, 1, 1, 0, 1, out) == 2
+    assert L.cudasph_gravity_plan(4096, 1, 1, 2, 2, out) == 2  # rank >= world
+    assert L.cudasph_gravity_plan(4096, 1, 1, 0, 0, out) == 2
+    assert L.cudasph_gravity_plan(4096, 7, 1, 0, 1, out) == 2  # precision
+    assert L.cudasph_gravity_plan(4096, 1, 5, 0, 1, out) == 2  # softening
+    assert L.cudasph_gravity_plan(4096, 1, 1, 0, 1, None) == 2
+    assert L.cudasph_gravity_plan(4096, 1, 1, 0, 1, out) == 0
+    tile, block, b0, b1, i0, i1, nt, chunk = list(out)
+    assert tile == 1024 and nt == 4 and b0 == 0 and b1 * block >= 4096 and i0 == 0 and i1 > 0
+    r, a, b = C.c_int(), C.c_int(), C.c_int()
+    assert L.cudasph_gravity_item(4096, -1, C.byref(r), C.byref(a), C.byref(b)) == 2
+    assert L.cudasph_gravity_item(4096, i1, C.byref(r), C.byref(a), C.byref(b)) == 2
+    assert L.cudasph_gravity_item(4096, 0, None, C.byref(a), C.byref(b)) == 2
+    assert L.cudasph_gravity_item(4096, 0, C.byref(r), C.byref(a), C.byref(b)) == 0
+    assert r.value == 0 and a.value == 1 and b.value > a.value
