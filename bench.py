@@ -235,13 +235,18 @@ SPH_BYTES = {
 SPH_GATHER = {"density": 64, "hydro": 96}
 
 
-def sph_bandwidth(ph, steps, n, nbar):
+def sph_bandwidth(ph, steps, n, nbar, l2_gbs=None):
     """Achieved HBM bandwidth of the bandwidth-bound phases (device time per
     step from the CUDA-event phase timers) against the measured copy peak,
     and the rate at which the pair loops gather neighbour records from L1/L2
-    (no measured L2 peak on this pool: reported as a rate only)."""
+    against the L2 read rate measured in the same run (cudasph_l2_peak; the
+    pool's peaks file has no L2 figure).  L1 hits can lift a gather rate above
+    the L2 figure."""
     peak, src = measured_hbm_gbs()
     out = {"peak_gbs": peak, "peak_source": src, "mean_neighbours": nbar}
+    if l2_gbs:
+        out["l2_read_gbs"] = round(l2_gbs, 1)
+        out["l2_source"] = "L2 read probe in this run (48 MB resident buffer, 32-byte L2-only loads from every SM)"
     for k, f in SPH_BYTES.items():
         if k not in ph or ph[k][0] <= 0:
             continue
@@ -250,7 +255,10 @@ def sph_bandwidth(ph, steps, n, nbar):
         out[k] = {"ms": round(ms, 4), "bytes_per_particle": round(f(nbar), 1), "gbs": round(b / (ms * 1e-3) / 1e9, 1),
                   "frac": round(b / (ms * 1e-3) / 1e9 / peak, 4)}
         if k in SPH_GATHER:
-            out[k]["gather_gbs"] = round(SPH_GATHER[k] * nbar * n / (ms * 1e-3) / 1e9, 1)
+            g = SPH_GATHER[k] * nbar * n / (ms * 1e-3) / 1e9
+            out[k]["gather_gbs"] = round(g, 1)
+            if l2_gbs:
+                out[k]["gather_frac_of_l2"] = round(g / l2_gbs, 4)
     return out
 
 
@@ -737,6 +745,7 @@ def run_ours(args, rank, world):
     L = _capi.lib()
     peak32 = L.cudasph_fma_peak(1, 4096, None)
     peak64 = L.cudasph_fma_peak(0, 1024, None)
+    l2_gbs = L.cudasph_l2_peak(200, None) / 1e9
 
     # --- the mixed (headline) step -------------------------------------------------
     sim = Simulation(ic, make_params(**kw), device=dev)
@@ -786,7 +795,7 @@ def run_ours(args, rank, world):
                        "flops_per_launch": flops, "launch_ms": grav_ms,
                        "interactions_per_s": n * n / (grav_ms * 1e-3)}
     out["stats_last_step"] = {k: stats[k] for k in ("E", "W", "T", "U", "dt", "ngb_mean", "ngb_min", "ngb_max")}
-    out["sph_roofline"] = sph_bandwidth(ph, args.steps, n, stats["ngb_mean"])
+    out["sph_roofline"] = sph_bandwidth(ph, args.steps, n, stats["ngb_mean"], l2_gbs if l2_gbs > 0 else None)
 
     # --- FP64 comparison and errors ----------------------------------------------
     first = {}  # tree-order fields after the first step of each form (the oracle check below)

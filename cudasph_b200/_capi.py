@@ -94,6 +94,8 @@ def lib():
     L.cudasph_gravity_direct.argtypes = [ip, vp, vp, vp, ip, dp, dp, ip, vp]
     L.cudasph_fma_peak.argtypes = [ip, ip, vp]
     L.cudasph_fma_peak.restype = C.c_double
+    L.cudasph_l2_peak.argtypes = [ip, vp]
+    L.cudasph_l2_peak.restype = C.c_double
     L.cudasph_set_keep.argtypes = [vp, ip]
     L.cudasph_set_graph.argtypes = [vp, ip]
     L.cudasph_adjoint_set_field.argtypes = [vp, ip, vp, ip]

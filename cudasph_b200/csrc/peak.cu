@@ -92,3 +92,68 @@ extern "C" double cudasph_fma_peak(int precision, int iters, void *stream) {
   cudaStreamSynchronize(st);
   return best;
 }
+
+namespace sph {
+
+// L2 read-bandwidth probe: a 48 MB buffer (well inside the 126 MB L2, after
+// a first pass that brings it there) read by every SM in a grid-stride loop,
+// 32 bytes per load, cached at L2 only (ld.global.cg), so the figure is the
+// L2-to-SM read rate: the denominator of the gather rates of the neighbour
+// loops, whose records come from L1 and L2.
+__global__ void __launch_bounds__(256) k_l2_read(const double4 *__restrict__ buf, long long n4, int iters,
+                                                 double *out) {
+  double acc = 0;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (int it = 0; it < iters; it++) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4; i += stride) {
+      double4 v;
+      asm volatile("ld.global.cg.v4.f64 {%0, %1, %2, %3}, [%4];"
+                   : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(v.w)
+                   : "l"(buf + i));
+      acc += (v.x + v.y) + (v.z + v.w);
+    }
+  }
+  if (acc == -1.2345) out[0] = acc;  // keeps the loads alive
+}
+
+}  // namespace sph
+
+// Runs the L2 probe on `stream` and returns the achieved read bytes/s
+// (CUDA events, the better of two timed launches after a warm-up).
+extern "C" double cudasph_l2_peak(int iters, void *stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long bytes = 48ll << 20, n4 = bytes / 32;
+  if (iters < 1) return -1;
+  void *buf = nullptr, *out = nullptr;
+  if (cudaMallocAsync(&buf, (size_t)bytes, st) != cudaSuccess) return -1;
+  if (cudaMallocAsync(&out, sizeof(double), st) != cudaSuccess) {
+    cudaFreeAsync(buf, st);
+    return -1;
+  }
+  cudaMemsetAsync(buf, 0, (size_t)bytes, st);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int blocks = sms * 8, threads = 256;
+  sph::k_l2_read<<<blocks, threads, 0, st>>>((const double4 *)buf, n4, 1, (double *)out);  // into L2
+  double best = -1;
+  for (int rep = 0; rep < 2; rep++) {
+    cudaEventRecord(e0, st);
+    sph::k_l2_read<<<blocks, threads, 0, st>>>((const double4 *)buf, n4, iters, (double *)out);
+    cudaEventRecord(e1, st);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    const double r = ms > 0 ? (double)bytes * iters / (ms * 1e-3) : -1;
+    if (r > best) best = r;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFreeAsync(buf, st);
+  cudaFreeAsync(out, st);
+  cudaStreamSynchronize(st);
+  return best;
+}

@@ -324,6 +324,11 @@ int cudasph_gravity_direct(int n, const double *pos4, const double *range, doubl
  * FP32, 0 = FP64.  The roofline denominator of the direct-N gravity loop. */
 double cudasph_fma_peak(int precision, int iters, void *stream);
 
+/* L2 read-bandwidth probe (bytes/s): a 48 MB buffer, resident in L2 after a
+ * first pass, read `iters` times by every SM with 32-byte L2-only loads, on
+ * `stream`.  The denominator of the neighbour loops' gather rates. */
+double cudasph_l2_peak(int iters, void *stream);
+
 /* ---------------------------------------------------------------------- */
 /* the reference's extern "C" boundary (CUDAsph.h:22-48)                   */
 /* ---------------------------------------------------------------------- */
