@@ -924,7 +924,7 @@ def run_ours(args, rank, world):
 def run_sharded(args, rank, world):
     """N > 1 ranks under torchrun: ONE simulation of n particles sharded over
     the ranks (cudasph_b200.sharded: leaf ranges of the SPH loops and shares
-    of the gravity work items per rank, three NCCL all-reduces per step), so
+    of the gravity work items per rank, an all-gather and two all-reduces per step), so
     the total work is fixed as N grows (strong scaling).  Device time: CUDA
     events on each rank's context stream around the timed steps (collectives
     included), max over ranks."""
@@ -1003,7 +1003,7 @@ def run_sharded(args, rank, world):
                       "precision": "fp64" if args.fp64_only else "mixed (FP32 gravity pair terms, FP64 SPH pair terms)",
                       "l2": "state (~%.0f MB) larger than L2; no flush" % (n * 500 / 1e6),
                       "parallelism": f"shard{world}: SPH leaf ranges + gravity work items per rank, replicated "
-                                     f"state, 3 NCCL all-reduces per step"},
+                                     f"state, per step an all-gather (density exchange) and two all-reduces (NCCL)"},
            "gpu_launches": int(launches),
            "phase_ms_per_step": {k: round(v[0] / args.steps, 4) for k, v in ph.items()},
            "exchange_and_gaps_ms_per_step": round(ms_local - phase_sum, 4),
