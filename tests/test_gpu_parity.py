@@ -257,6 +257,27 @@ def test_whole_steps_fp64_match_oracle():
     assert abs(st["time"] - ref.time) < 1e-15
 
 
+@pytest.mark.parametrize("n", [40, 97, 1000, 2049])
+def test_whole_steps_small_and_ragged_n_match_oracle(n):
+    """Whole FP64 steps at sizes that reach the edges of the layout: a tree
+    of one or two levels, a last leaf of fewer than 32 particles, a single
+    gravity tile (the one-sided blocks then cover every pair) or one tile
+    and a single particle beyond it, and a queue of resumed h-solve leaves
+    that holds one leaf or none."""
+    ic = ics.polytrope(n, n_ngb=24, seed=40 + n)
+    kw = dict(n_target=24.0, eos_mode=1, soft_mode=1, eps=0.01)
+    sim = _sim(ic, **kw)
+    ref = O.Sim(ic, O.make_params(**kw))
+    for _ in range(3):
+        sim.step()
+        ref.step()
+    for k in ("x", "vx", "u", "range", "rho", "P", "ax", "du", "phi"):
+        assert _rel(sim.get(k), ref.arr[k]) < 1e-8, (n, k)
+    assert np.array_equal(sim.n_ngb(), ref.n_ngb)
+    assert sim.device_status() & 0x7 == 0
+    sim.close()
+
+
 def test_graph_replay_matches_eager_steps():
     ic = ics.polytrope(5000, n_ngb=50, seed=9)
     kw = dict(n_target=50.0, eos_mode=1, soft_mode=1, eps=0.01, precision=1)
