@@ -410,8 +410,10 @@ __global__ void __launch_bounds__(kGThreads) k_grav_f32x2_plummer(int n, const d
 // go to the eight i-pairs a lane carries: many independent pairs per lane
 // hide the MUFU and shuffle latencies better than more resident warps, as a
 // sweep of warps x i-pairs per lane at N = 1M showed: 2 x 8 took 357 ms,
-// 4 x 5 360 ms, 4 x 4 371 ms, 8 x 2 with FP64 registers 412 ms) and are
-// added to the output at the end of the item.
+// 4 x 5 360 ms, 4 x 4 371 ms, 8 x 2 with FP64 registers 412 ms; later, with
+// the equal-mass form, 2 x 8 at 248 registers took 315 ms and 2 x 6 at 168
+// registers, six blocks per SM, 327 ms) and are added to the output at the
+// end of the item.
 // The output therefore holds the diagonal-tile sums first (stored by the
 // one-sided kernel) and receives the off-diagonal sums by atomics, so the
 // order of the FP64 additions, not their values, varies between runs.
