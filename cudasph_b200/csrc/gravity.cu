@@ -413,7 +413,9 @@ __global__ void __launch_bounds__(kGThreads) k_grav_f32x2_plummer(int n, const d
 // 4 x 5 360 ms, 4 x 4 371 ms, 8 x 2 with FP64 registers 412 ms; later, with
 // the equal-mass form, 2 x 8 at 248 registers took 315 ms and 2 x 6 at 168
 // registers, six blocks per SM, 327 ms) and are added to the output at the
-// end of the item.
+// end of the item.  The FMA pipe is the limiter; moving work to the MUFU
+// pipe does not pay: s^-2 from a MUFU reciprocal instead of a multiply for
+// 2, 4 or 8 of the 8 i-pairs measured 308, 312 and 330 ms against 303.
 // The output therefore holds the diagonal-tile sums first (stored by the
 // one-sided kernel) and receives the off-diagonal sums by atomics, so the
 // order of the FP64 additions, not their values, varies between runs.
