@@ -138,4 +138,7 @@ def test_step_gravity_equal_mass_form(precision, equal):
         rms = lambda x, y: np.sqrt(np.mean(np.sum((x - y) ** 2, 1)) / np.mean(np.sum(y ** 2, 1)))
         assert rms(a, r) < 1e-6
         assert rms(a, g) < 1e-6
+        # the equal-mass form's padding sources carry no potential weight:
+        # their 1/s of about 1e-18 must not show in any particle's potential
+        assert np.max(np.abs(got[:, 3] / ref[:, 3] - 1)) < 1e-6
         assert np.max(np.abs(got[:, 3] / ref[:, 3] - 1)) < 1e-5
