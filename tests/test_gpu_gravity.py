@@ -11,6 +11,7 @@ mode) on the same particles.
 import numpy as np
 import pytest
 
+from oracle import known_answers as KA
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -141,4 +142,36 @@ def test_step_gravity_equal_mass_form(precision, equal):
         # the equal-mass form's padding sources carry no potential weight:
         # their 1/s of about 1e-18 must not show in any particle's potential
         assert np.max(np.abs(got[:, 3] / ref[:, 3] - 1)) < 1e-6
-        assert np.max(np.abs(got[:, 3] / ref[:, 3] - 1)) < 1e-5
+
+
+# Isolated pairs through the standalone gravity entry against the closed-form
+# softened law (oracle/known_answers.py): Plummer and the spline softening at
+# the ranges 0.2 and 0.3, in every regime of r (inner and outer polynomial of
+# each range, between them, beyond both) and for coincident particles.  FP64
+# to the 12-decimal constants of the spline polynomials; mixed to FP32.
+PAIR_SEPARATIONS = [0.0, 0.01, 0.05, 0.099, 0.101, 0.149, 0.151, 0.199, 0.201, 0.25, 0.299, 0.301, 0.6]
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-11), (1, 1e-5)])
+@pytest.mark.parametrize("soft_mode", [0, 1])
+def test_isolated_pair_follows_the_softening_law(soft_mode, precision, tol):
+    import torch
+    from cudasph_b200._capi import lib
+    eps, G = 0.05, 1.3
+    st = torch.cuda.current_stream().cuda_stream
+    for r in PAIR_SEPARATIONS:
+        pos, m, rng, acc, phi = KA.two_body(r, soft_mode=soft_mode, eps=eps, G=G)
+        src = torch.from_numpy(np.column_stack([pos, m]).copy()).cuda()
+        ranges = torch.from_numpy(rng.copy()).cuda()  # the entry squares them on the device
+        out = torch.full((2, 4), np.nan, dtype=torch.float64, device="cuda")
+        rc = lib().cudasph_gravity_direct(2, src.data_ptr(), ranges.data_ptr() if soft_mode == 0 else None,
+                                          out.data_ptr(), soft_mode, eps, G, precision, st)
+        assert rc == 0
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        assert np.all(np.isfinite(got)), r
+        if r == 0.0:
+            assert np.all(got[:, :3] == 0.0)
+        else:
+            assert np.max(np.abs(got[:, :3] - acc)) <= tol * np.max(np.abs(acc)), (r, got[:, :3], acc)
+        assert np.max(np.abs(got[:, 3] / phi - 1)) <= tol, (r, got[:, 3], phi)
