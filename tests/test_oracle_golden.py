@@ -189,6 +189,34 @@ def test_isolated_pair_gravity_follows_the_softening_law(soft_mode):
         assert np.max(np.abs(g[3] / phi - 1)) <= 1e-11, r
 
 
+# The density of an n = 1 polytrope against the analytic Lane-Emden profile
+# rho = rho_c sin(pi r) / (pi r), rho_c = pi M / (4 R^3) (M = R = G = 1): the
+# h solve, the neighbour sets and the density loop of the oracle on the seeded
+# star, inside r < 0.7 (the kernel's truncation at the surface biases the
+# outer shells low).  The SPH smoothing error is a bias of order h^2 (about
+# -1 % at 8,192 particles, -0.7 % at 16,384), so it must also shrink with
+# the ranges as h^2 when the resolution doubles.
+def test_density_of_an_n1_polytrope_converges_to_lane_emden():
+    from cudasph_b200 import ics
+    p = O.make_params(n_target=50.0, eos_mode=0, soft_mode=1, eps=0.01, rel_err=1e-6, max_iter=40)
+    bias, h = [], []
+    for n in (8192, 16384):
+        ic = ics.polytrope(n, n_poly=1.0, n_ngb=50.0, seed=3)
+        rng, _, _ = O.solve_range(ic["x"], ic["y"], ic["z"], ic["range"], p)
+        cnt, off, lst = O.find_ngb(ic["x"], ic["y"], ic["z"], rng)
+        s = {k: ic[k] for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+        s["range"] = rng
+        rho = O.density(s, off, lst)["rho"]
+        r = np.sqrt(ic["x"] ** 2 + ic["y"] ** 2 + ic["z"] ** 2)
+        inner = r < 0.7
+        rel = rho[inner] / (np.pi / 4 * np.sinc(r[inner])) - 1  # np.sinc(x) = sin(pi x) / (pi x)
+        assert abs(rel.mean()) < 0.015 and np.sqrt(np.mean(rel ** 2)) < 0.02, (n, rel.mean())
+        bias.append(rel.mean())
+        h.append(rng[inner].mean())
+    expect = (h[1] / h[0]) ** 2
+    assert abs(bias[1] / bias[0] - expect) < 0.25 * expect, (bias, h)
+
+
 def test_peano_hilbert_key_against_reference(tab):
     """peano_hilbert_key (sort_bodies.cpp:66-105): the 200 keys the reference
     made for random 18-bit triplets, bit for bit, and the curve's defining
