@@ -184,11 +184,12 @@ def rms_rel(a, b):
 
 def traffic_from_profiles(kernel_tag: str, n: int):
     """Per-launch DRAM bytes of a kernel from the committed ncu summary
-    (profiles/<kernel_tag>.md, line 'traffic_bytes_per_launch_at_N=<n0>: <B>'),
-    scaled to n in proportion to the particles: the 32-byte source records
-    and the 32-byte output records the pair kernel accumulates into (64 MB at
-    N = 1M) stay resident in L2 across the N^2 interactions, so DRAM sees each
-    record once per launch."""
+    (profiles/<kernel_tag>.md, line 'traffic_bytes_per_launch_at_N=<n0>: <B>';
+    for the mixed gravity kernel captured at the bench size itself, N = 1M),
+    scaled to n in proportion to the particles when n differs: the 32-byte
+    source records and the 32-byte output records the pair kernel accumulates
+    into (64 MB at N = 1M) stay resident in L2 across the N^2 interactions,
+    so DRAM sees each record about once per launch."""
     path = os.path.join(ROOT, "profiles", kernel_tag + ".md")
     if not os.path.exists(path):
         return None
